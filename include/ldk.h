@@ -1,0 +1,132 @@
+/*
+ * libldk -- B200 (sm_100a) two-locus LD parse: SNP pairs within a distance cutoff ->
+ * per-population two-locus counts -> unbiased DD / Dz / pi2 and r^2 estimators ->
+ * distance-bin sums.  C ABI: plain pointers and sizes, no exceptions, no allocation.
+ *
+ * All array arguments are DEVICE pointers unless marked "host".  Every entry point
+ * returns LDK_OK (0) or a negative status; ldk_last_error() gives the message of the
+ * calling host thread's last failure.  Work is enqueued on `stream` (a cudaStream_t,
+ * NULL = legacy default stream).  Entry points that report device-side status read a
+ * 4-byte status word back (a stream synchronisation) before returning.
+ *
+ * References are to pg_gpu (the drop-in target): file:line within that project.
+ */
+#ifndef LDK_H
+#define LDK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define LDK_API __attribute__((visibility("default")))
+#else
+#define LDK_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LDK_OK 0
+#define LDK_ERR_ARG (-1)         /* invalid argument (null pointer, bad size, unsorted) */
+#define LDK_ERR_CUDA (-2)        /* CUDA runtime error */
+#define LDK_ERR_ARCH (-3)        /* device is not sm_100 (B200/GB200) */
+#define LDK_ERR_WORKSPACE (-4)   /* caller workspace smaller than ldk_*_workspace_size */
+#define LDK_ERR_DEVICE (-5)      /* device status word set (timeout, block range, bad code) */
+#define LDK_ERR_UNSUPPORTED (-6) /* configuration outside the kernels' limits */
+
+#define LDK_MAX_POPS 4
+#define LDK_MAX_BINS 64
+
+/* counting / estimator method of ldk_parse */
+#define LDK_METHOD_PLAIN_FP64 0 /* per-pair byte counting + FP64 estimators (the drop-in) */
+#define LDK_METHOD_TC 1         /* INT8 tcgen05 Gram counts + FP32 estimators, FP64 bins */
+
+LDK_API int ldk_version(void);
+LDK_API const char* ldk_last_error(void);
+
+/* Per-pair haplotype counts [n11, n10, n01, n00] and valid-pair counts over the rows
+ * `rows[0..n_rows)` of X (n_total_rows x ld_x int8 in {0, 1, -1}).
+ * Replaces ld_pipeline.compute_counts_for_pairs (ld_pipeline.py:130-175). */
+LDK_API int ldk_counts_hap(const int8_t* X, int64_t ld_x, int64_t n_var, const int32_t* rows,
+                   int32_t n_rows, const int32_t* idx_i, const int32_t* idx_j, int64_t n_pairs,
+                   int32_t* counts, int32_t* n_valid, void* stream);
+
+/* Per-pair nine-cell genotype counts (column g_i*3 + g_j) and valid counts, X in
+ * {0, 1, 2, -1}.  Replaces ld_pipeline.compute_genotype_counts_for_pairs and its
+ * _GENO_COUNTS_KERN (ld_pipeline.py:183-263). */
+LDK_API int ldk_counts_geno(const int8_t* X, int64_t ld_x, int64_t n_var, const int32_t* rows,
+                    int32_t n_rows, const int32_t* idx_i, const int32_t* idx_j, int64_t n_pairs,
+                    int32_t* counts, int32_t* n_valid, void* stream);
+
+/* Moments-ordered statistics (n_pairs x n_stats, float64) of P populations from
+ * per-population counts: counts (P, n_pairs, 4) [haplotype] or (P, n_pairs, 9)
+ * [genotype] int32, n_valid (P, n_pairs) int32 or NULL.
+ * Replaces compute_multi_pop_statistics_batch_hap (haplotype_kernels.py:584-640),
+ * compute_multi_pop_statistics_batch_geno (genotype_kernels.py:881-936) and
+ * compute_two_pop_statistics_batch (ld_pipeline.py:271-322). */
+LDK_API int ldk_stats(int genotypes, int P, const int32_t* counts, const int32_t* n_valid,
+              int64_t n_pairs, double* out, void* stream);
+
+/* One raw haplotype estimator call on float64 counts (n_pairs, 4*P_total) with
+ * n_valid (n_pairs, P_total) or NULL.  case_id and args are the canonical case of
+ * the call (see pg_gpu_b200/csrc/gen_estimators.py: RAW_CASES); out is n_pairs.
+ * Replaces the per-case kernels behind ld_statistics.dd / dz / pi2
+ * (ld_statistics.py:13-129, haplotype_kernels.py:69-304). */
+LDK_API int ldk_raw_hap(int case_id, const int32_t* args_host, int P_total, const double* counts,
+                const double* n_valid, int64_t n_pairs, double* out, void* stream);
+
+/* r (which=0), r^2 (1) or D' (2) per pair from float64 counts (n_pairs, 4) and n_valid
+ * or NULL.  Replaces ld_statistics.r / r_squared / d_prime (ld_statistics.py:153-246,
+ * haplotype_kernels.py:20-62). */
+LDK_API int ldk_r_family(int which, const double* counts, const double* n_valid, int64_t n_pairs,
+                 double* out, void* stream);
+
+/* The binned parse: every pair i < j of one window with pos[j] - pos[i] <= max_dist,
+ * binned by |coord[j] - coord[i]| into right-open bins, summed per bootstrap block of
+ * its left SNP.  Replaces the loop body of moments_ld._compute_ld_sums
+ * (moments_ld.py:309-341) and of HaplotypeMatrix.compute_ld_statistics_gpu_single_pop /
+ * _two_pops (haplotype_matrix.py:1657-1689, 1789-1837). */
+typedef struct {
+    const int8_t* X;            /* (n_rows, ld_x) int8: haplotypes {0,1,-1} or genotypes {0,1,2,-1} */
+    int64_t ld_x;               /* row stride of X in elements (>= n_var) */
+    int64_t n_rows;
+    int64_t n_var;
+    int32_t genotypes;          /* 0: haplotype path (4 counts), 1: genotype path (9 counts) */
+    int32_t n_pops;             /* P in 1..4 */
+    const int32_t* pop_rows;    /* concatenated row indices of the P populations */
+    int32_t pop_offsets[LDK_MAX_POPS + 1]; /* host: population p = pop_rows[off[p]..off[p+1]) */
+    const double* pos;          /* (n_var) positions, non-decreasing within each window */
+    const double* coord;        /* (n_var) binning coordinate (e.g. Morgans) or NULL = pos */
+    double max_dist;            /* pair cutoff on pos */
+    int32_t n_bins;             /* 1..64 */
+    double edges[LDK_MAX_BINS + 1]; /* host: increasing bin edges */
+    const int64_t* window_offsets; /* host (n_windows + 1) SNP ranges, or NULL = one window */
+    int32_t n_windows;
+    const int32_t* snp_block;   /* (n_var) bootstrap block of each SNP, or NULL = all 0 */
+    int32_t n_blocks;           /* >= 1 */
+    int32_t method;             /* LDK_METHOD_* */
+} ldk_parse_t;
+
+typedef struct {
+    double* sums;        /* (n_blocks, n_bins, n_stats) statistic sums */
+    double* r2_sums;     /* (n_blocks, n_bins) sum of finite r^2 of population 0 (dosage r^2 on the genotype path) */
+    uint64_t* pairs;     /* (n_blocks, n_bins) pairs binned */
+    uint64_t* r2_counts; /* (n_blocks, n_bins) pairs with finite r^2 */
+} ldk_parse_out_t;
+
+LDK_API int ldk_n_stats(int P);   /* 3, 15, 45, 105 */
+LDK_API size_t ldk_parse_workspace_size(const ldk_parse_t* d);
+LDK_API int ldk_parse(const ldk_parse_t* d, const ldk_parse_out_t* out, void* workspace,
+              size_t workspace_bytes, void* stream);
+
+/* out[r, k] = sum_b weights[r, b] * block_sums[b, k] (float64); weights int32 (R, n_blocks).
+ * Block-bootstrap replicates over pre-binned per-block sums, the semantics of
+ * resampling.block_bootstrap (resampling.py:201-256); also per-window totals. */
+LDK_API int ldk_block_combine(const double* block_sums, int64_t n_blocks, int64_t k,
+                      const int32_t* weights, int64_t n_rep, double* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LDK_H */

@@ -717,12 +717,15 @@ def geno_dosage_r2(counts9):
 
 
 def bin_sums(data, positions, pop_rows, edges, genotypes=False, chunk=200_000,
-             max_dist=None, coords=None, pair_range=None):
+             max_dist=None, coords=None, pair_range=None, window_offsets=None,
+             snp_block=None, n_blocks=1):
     """Per-bin sums of the moments-ordered statistics.
 
-    Returns dict: ``sums`` (n_bins, n_stats), ``pairs`` (n_bins,) pairs per bin,
-    ``r2_sum`` / ``r2_count`` (n_bins,) over pairs with finite r^2 (first population;
-    dosage r^2 on the genotype path), and ``n_pairs`` (pairs generated, incl. dropped).
+    Returns dict: ``sums`` (n_blocks, n_bins, n_stats), ``pairs`` (n_blocks, n_bins)
+    pairs per bin, ``r2_sum`` / ``r2_count`` (n_blocks, n_bins) over pairs with finite
+    r^2 (first population; dosage r^2 on the genotype path), and ``n_pairs`` (pairs
+    generated, incl. dropped).  ``window_offsets`` restricts pairs to SNP windows;
+    ``snp_block`` assigns each pair to the bootstrap block of its left SNP.
 
     ``coords`` (optional, per-SNP f64) replaces positions for binning, as the
     genetic-map path does (moments_ld.py:301-311); the pair cutoff still uses
@@ -734,11 +737,23 @@ def bin_sums(data, positions, pop_rows, edges, genotypes=False, chunk=200_000,
     Pn = len(pop_rows)
     n_stats = len(ld_names(Pn))
     max_dist = float(edges[-1]) if max_dist is None else float(max_dist)
-    ii, jj = pairs_within_distance(positions, max_dist)
+    positions = np.asarray(positions)
+    if window_offsets is None:
+        window_offsets = [0, len(positions)]
+    iis, jjs = [], []
+    for a, b in zip(window_offsets[:-1], window_offsets[1:]):
+        ii, jj = pairs_within_distance(positions[a:b], max_dist)
+        iis.append(ii + a)
+        jjs.append(jj + a)
+    ii = np.concatenate(iis) if iis else np.empty(0, np.int64)
+    jj = np.concatenate(jjs) if jjs else np.empty(0, np.int64)
     if pair_range is not None:
         ii, jj = ii[pair_range[0]:pair_range[1]], jj[pair_range[0]:pair_range[1]]
-    out = {"sums": np.zeros((nb, n_stats)), "pairs": np.zeros(nb, np.int64),
-           "r2_sum": np.zeros(nb), "r2_count": np.zeros(nb, np.int64), "n_pairs": len(ii)}
+    blk_of = (np.zeros(len(positions), np.int64) if snp_block is None
+              else np.asarray(snp_block, np.int64))
+    out = {"sums": np.zeros((n_blocks, nb, n_stats)), "pairs": np.zeros((n_blocks, nb), np.int64),
+           "r2_sum": np.zeros((n_blocks, nb)), "r2_count": np.zeros((n_blocks, nb), np.int64),
+           "n_pairs": len(ii)}
     coord = np.asarray(positions if coords is None else coords, dtype=np.float64)
     count_fn = geno_counts if genotypes else hap_counts
     stat_fn = geno_stats if genotypes else hap_stats
@@ -753,14 +768,14 @@ def bin_sums(data, positions, pop_rows, edges, genotypes=False, chunk=200_000,
             nl.append(nv)
         st = stat_fn(cl, nl)
         keep = (cb >= 0) & (cb < nb)
-        vb = cb[keep]
-        np.add.at(out["sums"], vb, st[keep])
-        out["pairs"] += np.bincount(vb, minlength=nb)
+        flat = blk_of[ci[keep]] * nb + cb[keep]
+        np.add.at(out["sums"].reshape(-1, n_stats), flat, st[keep])
+        out["pairs"] += np.bincount(flat, minlength=n_blocks * nb).reshape(n_blocks, nb)
         r2 = geno_dosage_r2(cl[0]) if genotypes else hap_r_squared(cl[0], nl[0])
         r2 = r2[keep]
         fin = np.isfinite(r2)
-        np.add.at(out["r2_sum"], vb[fin], r2[fin])
-        out["r2_count"] += np.bincount(vb[fin], minlength=nb)
+        np.add.at(out["r2_sum"].reshape(-1), flat[fin], r2[fin])
+        out["r2_count"] += np.bincount(flat[fin], minlength=n_blocks * nb).reshape(n_blocks, nb)
     return out
 
 

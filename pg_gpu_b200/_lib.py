@@ -1,0 +1,121 @@
+"""ctypes binding of ``libldk.so`` (the C ABI in ``include/ldk.h``).
+
+There is no CPU fallback: every compute call goes through the CUDA library, and a
+missing library or a missing GPU raises immediately.  Device buffers are torch CUDA
+tensors; torch is used for allocation, streams and host/device copies only.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libldk.so")
+
+LDK_OK = 0
+LDK_ERR_ARG = -1
+LDK_ERR_CUDA = -2
+LDK_ERR_ARCH = -3
+LDK_ERR_WORKSPACE = -4
+LDK_ERR_DEVICE = -5
+LDK_ERR_UNSUPPORTED = -6
+MAX_POPS = 4
+MAX_BINS = 64
+METHOD_PLAIN = 0
+METHOD_TC = 1
+
+c_i8p = ctypes.c_void_p
+c_vp = ctypes.c_void_p
+
+
+class LdkError(RuntimeError):
+    """A libldk entry point returned a negative status."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"libldk error {code}: {msg}")
+        self.code = code
+
+
+class ParseDesc(ctypes.Structure):
+    """Mirror of ``ldk_parse_t``."""
+    _fields_ = [
+        ("X", c_vp), ("ld_x", ctypes.c_int64), ("n_rows", ctypes.c_int64), ("n_var", ctypes.c_int64),
+        ("genotypes", ctypes.c_int32), ("n_pops", ctypes.c_int32), ("pop_rows", c_vp),
+        ("pop_offsets", ctypes.c_int32 * (MAX_POPS + 1)), ("pos", c_vp), ("coord", c_vp),
+        ("max_dist", ctypes.c_double), ("n_bins", ctypes.c_int32),
+        ("edges", ctypes.c_double * (MAX_BINS + 1)), ("window_offsets", c_vp), ("n_windows", ctypes.c_int32),
+        ("snp_block", c_vp), ("n_blocks", ctypes.c_int32), ("method", ctypes.c_int32),
+    ]
+
+
+class ParseOut(ctypes.Structure):
+    """Mirror of ``ldk_parse_out_t``."""
+    _fields_ = [("sums", c_vp), ("r2_sums", c_vp), ("pairs", c_vp), ("r2_counts", c_vp)]
+
+
+EXPORTS = {
+    "ldk_version": (ctypes.c_int, []),
+    "ldk_last_error": (ctypes.c_char_p, []),
+    "ldk_n_stats": (ctypes.c_int, [ctypes.c_int]),
+    "ldk_counts_hap": (ctypes.c_int, [c_vp, ctypes.c_int64, ctypes.c_int64, c_vp, ctypes.c_int32, c_vp, c_vp,
+                                      ctypes.c_int64, c_vp, c_vp, c_vp]),
+    "ldk_counts_geno": (ctypes.c_int, [c_vp, ctypes.c_int64, ctypes.c_int64, c_vp, ctypes.c_int32, c_vp, c_vp,
+                                       ctypes.c_int64, c_vp, c_vp, c_vp]),
+    "ldk_stats": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, c_vp, c_vp, ctypes.c_int64, c_vp, c_vp]),
+    "ldk_raw_hap": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int32), ctypes.c_int, c_vp, c_vp,
+                                   ctypes.c_int64, c_vp, c_vp]),
+    "ldk_r_family": (ctypes.c_int, [ctypes.c_int, c_vp, c_vp, ctypes.c_int64, c_vp, c_vp]),
+    "ldk_parse_workspace_size": (ctypes.c_size_t, [ctypes.POINTER(ParseDesc)]),
+    "ldk_parse": (ctypes.c_int, [ctypes.POINTER(ParseDesc), ctypes.POINTER(ParseOut), c_vp, ctypes.c_size_t,
+                                 c_vp]),
+    "ldk_block_combine": (ctypes.c_int, [c_vp, ctypes.c_int64, ctypes.c_int64, c_vp, ctypes.c_int64, c_vp,
+                                         c_vp]),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load libldk and declare its signatures (no GPU needed to load)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `python -m pg_gpu_b200.build`")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in EXPORTS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc: int):
+    if rc != LDK_OK:
+        msg = load().ldk_last_error()
+        raise LdkError(rc, msg.decode() if msg else "")
+
+
+def require_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("pg_gpu_b200 needs a CUDA device (B200, sm_100a); no CPU fallback exists")
+    return torch
+
+
+def stream_handle(stream=None):
+    torch = require_cuda()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def ptr(t):
+    """Device pointer of a torch tensor (None -> NULL)."""
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return ctypes.c_void_p(t.data_ptr())

@@ -1,0 +1,310 @@
+// C ABI of libldk (declared in include/ldk.h).
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <algorithm>
+#include <vector>
+
+#include "ldk_internal.h"
+
+namespace ldk {
+
+namespace {
+thread_local char g_err[512] = "";
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+int stats_of(int P) { return P == 1 ? 3 : P == 2 ? 15 : P == 3 ? 45 : P == 4 ? 105 : 0; }
+
+int check_cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return LDK_OK;
+    set_error("%s: %s", what, cudaGetErrorString(e));
+    return LDK_ERR_CUDA;
+}
+
+// Device check: the library carries sm_100a code only.
+int check_arch() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        set_error("no CUDA device");
+        return LDK_ERR_CUDA;
+    }
+    int major = 0, minor = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+    if (major != 10 || minor != 0) {
+        set_error("libldk is built for sm_100a (B200); device %d is sm_%d%d", dev, major, minor);
+        return LDK_ERR_ARCH;
+    }
+    return LDK_OK;
+}
+
+struct Layout {
+    size_t status_off = 0, jmax_off = 0, win_off = 0, items_off = 0, hv_off = 0, total = 0;
+    int n_items = 0;
+};
+
+bool shape_of(const ldk_parse_t* d, ParseShape& sh) {
+    sh.P = d->n_pops;
+    sh.genotypes = d->genotypes;
+    sh.n_stats = stats_of(d->n_pops);
+    sh.n_bins = d->n_bins;
+    sh.planes = 2;
+    int k = 0;
+    for (int p = 0; p < LDK_MAX_POPS + 1; ++p) sh.kofs[p] = 0;
+    for (int p = 0; p < d->n_pops; ++p) {
+        sh.kofs[p] = k;
+        const int np = d->pop_offsets[p + 1] - d->pop_offsets[p];
+        k += (np + 31) / 32 * 32;
+    }
+    for (int p = d->n_pops; p <= LDK_MAX_POPS; ++p) sh.kofs[p] = k;
+    sh.ktot = (k + 127) / 128 * 128;
+    return true;
+}
+
+int window_count(const ldk_parse_t* d) { return d->window_offsets ? d->n_windows : 1; }
+
+int64_t window_bound(const ldk_parse_t* d, int w) {
+    if (d->window_offsets) return d->window_offsets[w];
+    return w == 0 ? 0 : d->n_var;
+}
+
+Layout layout_of(const ldk_parse_t* d, const ParseShape& sh) {
+    Layout L;
+    size_t off = 0;
+    L.status_off = off;
+    off += 256;
+    L.jmax_off = off;
+    off = align_up(off + (size_t)d->n_var * sizeof(int32_t), 256);
+    L.win_off = off;
+    off = align_up(off + (size_t)(window_count(d) + 1) * sizeof(int64_t), 256);
+    if (d->method == LDK_METHOD_TC) {
+        int n_items = 0;
+        for (int w = 0; w < window_count(d); ++w) {
+            const int64_t m = window_bound(d, w + 1) - window_bound(d, w);
+            n_items += (int)((m + 63) / 64);
+        }
+        L.n_items = n_items;
+        L.items_off = off;
+        off = align_up(off + (size_t)n_items * 2 * sizeof(int32_t), 1024);
+        L.hv_off = off;
+        off = align_up(off + (size_t)d->n_var * sh.planes * sh.ktot, 256);
+    }
+    L.total = off;
+    return L;
+}
+
+int validate(const ldk_parse_t* d) {
+    if (!d) { set_error("null descriptor"); return LDK_ERR_ARG; }
+    if (d->n_pops < 1 || d->n_pops > LDK_MAX_POPS) { set_error("n_pops must be 1..4"); return LDK_ERR_ARG; }
+    if (d->n_bins < 1 || d->n_bins > LDK_MAX_BINS) { set_error("n_bins must be 1..64"); return LDK_ERR_ARG; }
+    for (int b = 0; b < d->n_bins; ++b)
+        if (!(d->edges[b] < d->edges[b + 1])) { set_error("bin edges must increase"); return LDK_ERR_ARG; }
+    if (d->n_var < 0 || d->n_var > (int64_t)INT32_MAX - 1024) { set_error("n_var out of range"); return LDK_ERR_ARG; }
+    if (d->n_var > 0 && (!d->X || !d->pos || !d->pop_rows)) { set_error("null input pointer"); return LDK_ERR_ARG; }
+    if (d->ld_x < d->n_var) { set_error("ld_x < n_var"); return LDK_ERR_ARG; }
+    if (d->pop_offsets[0] != 0) { set_error("pop_offsets[0] must be 0"); return LDK_ERR_ARG; }
+    for (int p = 0; p < d->n_pops; ++p)
+        if (d->pop_offsets[p + 1] <= d->pop_offsets[p]) { set_error("empty population %d", p); return LDK_ERR_ARG; }
+    if (d->n_blocks < 1) { set_error("n_blocks must be >= 1"); return LDK_ERR_ARG; }
+    if (d->method != LDK_METHOD_PLAIN_FP64 && d->method != LDK_METHOD_TC) { set_error("unknown method"); return LDK_ERR_ARG; }
+    if (!(d->max_dist >= 0.0)) { set_error("max_dist must be >= 0"); return LDK_ERR_ARG; }
+    if (d->window_offsets) {
+        if (d->n_windows < 1) { set_error("n_windows must be >= 1"); return LDK_ERR_ARG; }
+        if (d->window_offsets[0] != 0 || d->window_offsets[d->n_windows] != d->n_var) {
+            set_error("window_offsets must run from 0 to n_var");
+            return LDK_ERR_ARG;
+        }
+        for (int w = 0; w < d->n_windows; ++w)
+            if (d->window_offsets[w + 1] < d->window_offsets[w]) { set_error("window_offsets must not decrease"); return LDK_ERR_ARG; }
+    }
+    if (d->method == LDK_METHOD_TC && d->genotypes) {
+        set_error("the tensor-core method covers the haplotype path; use LDK_METHOD_PLAIN_FP64 for genotypes");
+        return LDK_ERR_UNSUPPORTED;
+    }
+    return LDK_OK;
+}
+
+const char* status_text(unsigned s) {
+    if (s & LDK_DEVERR_TIMEOUT) return "device wait timed out";
+    if (s & LDK_DEVERR_BLOCK_RANGE) return "snp_block outside [0, n_blocks)";
+    if (s & LDK_DEVERR_BLOCK_SPAN) return "a 64-SNP row block spans more than two bootstrap blocks";
+    if (s & LDK_DEVERR_BAD_INPUT) return "unsorted positions or allele codes outside {-1, 0, 1}";
+    return "device error";
+}
+
+}  // namespace
+
+void set_error(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+}  // namespace ldk
+
+using namespace ldk;
+
+extern "C" {
+
+int ldk_version(void) { return 10000; }
+
+const char* ldk_last_error(void) { return g_err; }
+
+int ldk_n_stats(int P) { return stats_of(P); }
+
+int ldk_counts_hap(const int8_t* X, int64_t ld_x, int64_t n_var, const int32_t* rows, int32_t n_rows,
+                   const int32_t* idx_i, const int32_t* idx_j, int64_t n_pairs, int32_t* counts, int32_t* n_valid,
+                   void* stream) {
+    if (n_pairs < 0 || n_rows < 0 || ld_x < n_var) { set_error("bad sizes"); return LDK_ERR_ARG; }
+    if (n_pairs > 0 && (!X || !rows || !idx_i || !idx_j || !counts)) { set_error("null pointer"); return LDK_ERR_ARG; }
+    if (int rc = check_arch()) return rc;
+    return check_cuda(launch_counts(0, X, ld_x, rows, n_rows, idx_i, idx_j, n_pairs, counts, n_valid,
+                                    (cudaStream_t)stream), "ldk_counts_hap");
+}
+
+int ldk_counts_geno(const int8_t* X, int64_t ld_x, int64_t n_var, const int32_t* rows, int32_t n_rows,
+                    const int32_t* idx_i, const int32_t* idx_j, int64_t n_pairs, int32_t* counts, int32_t* n_valid,
+                    void* stream) {
+    if (n_pairs < 0 || n_rows < 0 || ld_x < n_var) { set_error("bad sizes"); return LDK_ERR_ARG; }
+    if (n_pairs > 0 && (!X || !rows || !idx_i || !idx_j || !counts)) { set_error("null pointer"); return LDK_ERR_ARG; }
+    if (int rc = check_arch()) return rc;
+    return check_cuda(launch_counts(1, X, ld_x, rows, n_rows, idx_i, idx_j, n_pairs, counts, n_valid,
+                                    (cudaStream_t)stream), "ldk_counts_geno");
+}
+
+int ldk_stats(int genotypes, int P, const int32_t* counts, const int32_t* n_valid, int64_t n_pairs, double* out,
+              void* stream) {
+    if (P < 1 || P > LDK_MAX_POPS || n_pairs < 0) { set_error("bad P or n_pairs"); return LDK_ERR_ARG; }
+    if (n_pairs > 0 && (!counts || !out)) { set_error("null pointer"); return LDK_ERR_ARG; }
+    if (int rc = check_arch()) return rc;
+    return check_cuda(launch_stats(genotypes, P, counts, n_valid, n_pairs, out, (cudaStream_t)stream), "ldk_stats");
+}
+
+int ldk_raw_hap(int case_id, const int32_t* args_host, int P_total, const double* counts, const double* n_valid,
+                int64_t n_pairs, double* out, void* stream) {
+    if (case_id < 0 || case_id > 14 || P_total < 1 || P_total > LDK_MAX_POPS || n_pairs < 0 || !args_host) {
+        set_error("bad raw-call arguments");
+        return LDK_ERR_ARG;
+    }
+    static const int arity[15] = {1, 2, 1, 2, 2, 2, 3, 1, 2, 3, 3, 4, 2, 2, 3};
+    int32_t g[4] = {0, 0, 0, 0};
+    for (int k = 0; k < arity[case_id]; ++k) {
+        if (args_host[k] < 0 || args_host[k] >= P_total) { set_error("population index out of range"); return LDK_ERR_ARG; }
+        g[k] = args_host[k];
+    }
+    if (n_pairs > 0 && (!counts || !out)) { set_error("null pointer"); return LDK_ERR_ARG; }
+    if (int rc = check_arch()) return rc;
+    return check_cuda(launch_raw_hap(case_id, g, P_total, counts, n_valid, n_pairs, out, (cudaStream_t)stream),
+                      "ldk_raw_hap");
+}
+
+int ldk_r_family(int which, const double* counts, const double* n_valid, int64_t n_pairs, double* out, void* stream) {
+    if (which < 0 || which > 2 || n_pairs < 0) { set_error("bad arguments"); return LDK_ERR_ARG; }
+    if (n_pairs > 0 && (!counts || !out)) { set_error("null pointer"); return LDK_ERR_ARG; }
+    if (int rc = check_arch()) return rc;
+    return check_cuda(launch_r_family(which, counts, n_valid, n_pairs, out, (cudaStream_t)stream), "ldk_r_family");
+}
+
+size_t ldk_parse_workspace_size(const ldk_parse_t* d) {
+    if (validate(d) != LDK_OK) return 0;
+    ParseShape sh;
+    shape_of(d, sh);
+    return layout_of(d, sh).total;
+}
+
+int ldk_parse(const ldk_parse_t* d, const ldk_parse_out_t* out, void* workspace, size_t workspace_bytes,
+              void* stream) {
+    if (int rc = validate(d)) return rc;
+    if (!out || !out->sums || !out->r2_sums || !out->pairs || !out->r2_counts) {
+        set_error("null output pointer");
+        return LDK_ERR_ARG;
+    }
+    ParseShape sh;
+    shape_of(d, sh);
+    const Layout L = layout_of(d, sh);
+    if (!workspace || workspace_bytes < L.total) {
+        set_error("workspace of %zu bytes is smaller than the %zu required", workspace_bytes, L.total);
+        return LDK_ERR_WORKSPACE;
+    }
+    if (reinterpret_cast<uintptr_t>(workspace) % 256) { set_error("workspace must be 256-byte aligned"); return LDK_ERR_ARG; }
+    if (int rc = check_arch()) return rc;
+    if (d->method == LDK_METHOD_TC && tc_smem_bytes(sh) > 227 * 1024) {
+        set_error("bins x statistics exceed the tensor-core kernel's shared-memory staging");
+        return LDK_ERR_UNSUPPORTED;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned char* ws = static_cast<unsigned char*>(workspace);
+    Scratch w;
+    w.status = reinterpret_cast<unsigned*>(ws + L.status_off);
+    w.row_counter = reinterpret_cast<int*>(ws + L.status_off + 64);
+    w.jmax = reinterpret_cast<int32_t*>(ws + L.jmax_off);
+    w.win_off = reinterpret_cast<int64_t*>(ws + L.win_off);
+    w.items = reinterpret_cast<int32_t*>(ws + L.items_off);
+    w.hv = ws + L.hv_off;
+
+    const int nb = d->n_bins, NS = stats_of(d->n_pops);
+    int rc;
+    if ((rc = check_cuda(cudaMemsetAsync(out->sums, 0, sizeof(double) * d->n_blocks * nb * NS, s), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(out->r2_sums, 0, sizeof(double) * d->n_blocks * nb, s), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(out->pairs, 0, sizeof(uint64_t) * d->n_blocks * nb, s), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(out->r2_counts, 0, sizeof(uint64_t) * d->n_blocks * nb, s), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(ws + L.status_off, 0, 256, s), "memset")))
+        return rc;
+    if (d->n_var < 2) return LDK_OK;
+
+    std::vector<int64_t> woff(window_count(d) + 1);
+    for (int k = 0; k <= window_count(d); ++k) woff[k] = window_bound(d, k);
+    if ((rc = check_cuda(cudaMemcpyAsync(w.win_off, woff.data(), woff.size() * sizeof(int64_t),
+                                         cudaMemcpyHostToDevice, s), "upload windows")))
+        return rc;
+    ldk_parse_t dd = *d;
+    dd.n_windows = window_count(d);
+    if ((rc = check_cuda(launch_jmax(&dd, w, s), "pair ranges"))) return rc;
+
+    if (d->method == LDK_METHOD_PLAIN_FP64) {
+        if ((rc = check_cuda(launch_parse_plain(&dd, out, w, sh, s), "plain parse"))) return rc;
+    } else {
+        // row blocks of 64 SNPs, largest windows first (round-robin over persistent CTAs)
+        std::vector<int> order(window_count(d));
+        for (int k = 0; k < (int)order.size(); ++k) order[k] = k;
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+            return (woff[x + 1] - woff[x]) > (woff[y + 1] - woff[y]);
+        });
+        std::vector<int32_t> items;
+        items.reserve((size_t)L.n_items * 2);
+        for (int wi : order)
+            for (int64_t r0 = woff[wi]; r0 < woff[wi + 1]; r0 += 64) {
+                items.push_back((int32_t)r0);
+                items.push_back((int32_t)std::min<int64_t>(r0 + 64, woff[wi + 1]));
+            }
+        if (!items.empty() &&
+            (rc = check_cuda(cudaMemcpyAsync(w.items, items.data(), items.size() * sizeof(int32_t),
+                                             cudaMemcpyHostToDevice, s), "upload row blocks")))
+            return rc;
+        if ((rc = check_cuda(launch_prep_planes(&dd, w, sh, s), "indicator planes"))) return rc;
+        if ((rc = check_cuda(launch_parse_tc(&dd, out, w, sh, (int)(items.size() / 2), s), "tensor-core parse")))
+            return rc;
+    }
+    unsigned status = 0;
+    if ((rc = check_cuda(cudaMemcpyAsync(&status, w.status, sizeof(unsigned), cudaMemcpyDeviceToHost, s), "status")))
+        return rc;
+    if ((rc = check_cuda(cudaStreamSynchronize(s), "ldk_parse"))) return rc;
+    if (status) {
+        set_error("%s (status 0x%x)", status_text(status), status);
+        return LDK_ERR_DEVICE;
+    }
+    return LDK_OK;
+}
+
+int ldk_block_combine(const double* block_sums, int64_t n_blocks, int64_t k, const int32_t* weights, int64_t n_rep,
+                      double* out, void* stream) {
+    if (n_blocks < 0 || k < 0 || n_rep < 0) { set_error("bad sizes"); return LDK_ERR_ARG; }
+    if (n_rep * k > 0 && (!block_sums || !weights || !out)) { set_error("null pointer"); return LDK_ERR_ARG; }
+    if (int rc = check_arch()) return rc;
+    return check_cuda(launch_block_combine(block_sums, n_blocks, k, weights, n_rep, out, (cudaStream_t)stream),
+                      "ldk_block_combine");
+}
+
+}  // extern "C"

@@ -1,0 +1,57 @@
+// Internal host/device interface between the C ABI (ldk_api.cu) and the kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ldk.h"
+#include "ldk_common.cuh"
+
+namespace ldk {
+
+// Per-call device scratch carved out of the caller's workspace.
+struct Scratch {
+    unsigned* status;      // device status word (LDK_DEVERR_* bits)
+    int* row_counter;      // dynamic row-chunk counter of the plain parse
+    int32_t* jmax;         // (n_var) exclusive end of each SNP's partner range
+    int64_t* win_off;      // (n_windows + 1) window SNP offsets
+    uint8_t* hv;           // TC path: (n_var, planes, Ktot) indicator planes
+    int32_t* items;        // TC path: (n_items, 2) row blocks
+};
+
+struct ParseShape {
+    int P;
+    int genotypes;
+    int n_stats;
+    int n_bins;
+    int kofs[LDK_MAX_POPS + 1];  // TC path: K offset (bytes) of each population segment
+    int ktot;                    // TC path: total K bytes (multiple of 128)
+    int planes;                  // TC path: indicator planes per SNP (2 haplotype, 4 genotype)
+};
+
+// launchers (ldk_plain.cu)
+cudaError_t launch_counts(int genotypes, const int8_t* X, int64_t ld, const int32_t* rows, int n_rows,
+                          const int32_t* ii, const int32_t* jj, int64_t n, int32_t* counts,
+                          int32_t* n_valid, cudaStream_t s);
+cudaError_t launch_stats(int genotypes, int P, const int32_t* counts, const int32_t* n_valid, int64_t n,
+                         double* out, cudaStream_t s);
+cudaError_t launch_raw_hap(int case_id, const int32_t* args, int P_total, const double* counts,
+                           const double* n_valid, int64_t n, double* out, cudaStream_t s);
+cudaError_t launch_r_family(int which, const double* counts, const double* n_valid, int64_t n,
+                            double* out, cudaStream_t s);
+cudaError_t launch_jmax(const ldk_parse_t* d, const Scratch& w, cudaStream_t s);
+cudaError_t launch_parse_plain(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w,
+                               const ParseShape& sh, cudaStream_t s);
+cudaError_t launch_block_combine(const double* block_sums, int64_t n_blocks, int64_t k,
+                                 const int32_t* weights, int64_t n_rep, double* out, cudaStream_t s);
+
+// launchers (ldk_tc.cu)
+cudaError_t launch_prep_planes(const ldk_parse_t* d, const Scratch& w, const ParseShape& sh,
+                               cudaStream_t s);
+cudaError_t launch_parse_tc(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w,
+                            const ParseShape& sh, int n_items, cudaStream_t s);
+int tc_rows_per_block(const ParseShape& sh);
+size_t tc_smem_bytes(const ParseShape& sh);
+
+void set_error(const char* fmt, ...);
+
+}  // namespace ldk

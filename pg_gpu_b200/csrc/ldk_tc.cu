@@ -1,0 +1,638 @@
+// Tensor-core path of the binned parse (sm_100a).
+//
+// Counting as a Gram product.  For SNPs i, j and one population, with per-haplotype
+// indicators h = [allele == 1] and v = [allele != missing], the four products
+//   hh = sum_k h_ik h_jk,  hv = sum_k h_ik v_jk,  vh = sum_k v_ik h_jk,  vv = sum_k v_ik v_jk
+// give the two-locus counts exactly: n11 = hh, n10 = hv - hh, n01 = vh - hh,
+// n00 = vv - hv - vh + hh, n_valid = vv (pg_gpu ld_pipeline.py:155-172).
+//
+// Layout in HBM (built by k_prep_planes): per SNP two 0/1 byte planes (h, v) over the
+// concatenated haplotypes of all populations, each population padded to a multiple of
+// 32 bytes, the whole K axis to a multiple of 128 bytes:  planes[snp][plane][k].
+// A 3-D TMA box {128 k, 2 planes, R snps} then lands in shared memory as 2R interleaved
+// rows (h_i0, v_i0, h_i1, v_i1, ...) in the 128-byte-swizzled K-major layout that
+// tcgen05.mma reads directly.  One MMA per 32-byte K step and population:
+//   D[128 x 2NJ] (+)= A[128 rows = 64 SNPs x {h,v}] . B[2NJ rows = NJ SNPs x {h,v}]^T
+// with u8 inputs and s32 accumulation in tensor memory: TMEM lane 2r holds (hh, hv) and
+// lane 2r+1 holds (vh, vv) of SNP i0+r against every j of the tile.
+//
+// Warp roles (one CTA per SM, persistent over row blocks):
+//   warp 0     TMA producer (A: row block, B: 32..128 partner SNPs, per 128-byte K chunk)
+//   warp 1     TMEM allocator and single-thread MMA issuer, double-buffered accumulators
+//   warps 2-9  epilogue: tcgen05.ld the counts, swap halves between lane pairs, evaluate
+//              the FP32 estimators, sum per distance bin in registers (bins are monotone
+//              in j for a fixed i), stage per-bin FP64 sums in shared memory, add them to
+//              the per-bootstrap-block FP64 outputs once per row block.
+// Every wait is bounded (LDK_DEVERR_TIMEOUT) so a fault cannot hang the GPU.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "ldk_estimators.cuh"
+#include "ldk_internal.h"
+
+namespace ldk {
+
+namespace {
+
+constexpr int kRows = 64;               // SNPs per row block (M = 128 = 64 x {h, v})
+constexpr int kKChunk = 128;            // K bytes per TMA box / swizzle row
+constexpr int kEpiWarps = 8;            // two per TMEM lane quarter
+constexpr int kThreadsTC = 64 + 32 * kEpiWarps;
+constexpr int kSlots = 2;               // bootstrap blocks staged per row block
+constexpr int kTmemCols = 512;
+constexpr uint64_t kTimeoutNs = 5000000000ull;  // 5 s per wait
+
+template <int P>
+struct Cfg {
+    static constexpr int NJ = (P == 1) ? 128 : (P == 2) ? 64 : 32;  // partner SNPs per tile
+    static constexpr int N = 2 * NJ;                                 // MMA N
+    static constexpr int COLS = P * N;                               // TMEM columns per buffer
+    static constexpr int STAGES = (P == 1) ? 2 : (P == 2) ? 3 : 4;
+    static constexpr int A_BYTES = 2 * kRows * kKChunk;
+    static constexpr int B_BYTES = N * kKChunk;
+    static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+    static constexpr int NS = HapNStats<P>::value;
+    static_assert(2 * COLS <= kTmemCols, "TMEM budget");
+    static_assert(N % 16 == 0 && N <= 256, "MMA N");
+};
+
+// ---------------------------------------------------------------------------
+// PTX wrappers (tcgen05, TMA, mbarrier)
+// ---------------------------------------------------------------------------
+
+LDK_DEV uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+LDK_DEV void mbar_init(uint64_t* b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(b)), "r"(count));
+}
+LDK_DEV void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)), "r"(bytes) : "memory");
+}
+LDK_DEV void mbar_arrive(uint64_t* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
+}
+LDK_DEV bool mbar_test(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(su32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait on a barrier phase.  False on timeout or when another role aborted.
+LDK_DEV bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag, unsigned* status) {
+    if (mbar_test(b, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (;;) {
+        if (mbar_test(b, parity)) return true;
+        if (*abort_flag) return false;
+        if (global_ns() - t0 > kTimeoutNs) {
+            atomicOr(status, LDK_DEVERR_TIMEOUT);
+            *abort_flag = 1;
+            return false;
+        }
+    }
+}
+
+LDK_DEV void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1, int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(su32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(su32(bar)), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+
+LDK_DEV void tmem_alloc(uint32_t* dst, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(dst)), "r"(ncols));
+}
+LDK_DEV void tmem_relinquish() { asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;"); }
+LDK_DEV void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols));
+}
+LDK_DEV void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+LDK_DEV void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// K-major operand in the 128-byte swizzle layout: 8-row groups 1024 bytes apart.
+LDK_DEV uint64_t sw128_desc(uint32_t saddr) {
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;              // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;    // stride byte offset
+    d |= (uint64_t)1 << 46;              // descriptor version for sm_100
+    d |= (uint64_t)2 << 61;              // SWIZZLE_128B
+    return d;
+}
+
+// kind::i8 instruction descriptor: u8 x u8 -> s32, K-major A and B, M = 128.
+template <int N>
+__host__ __device__ constexpr uint32_t idesc_u8() {
+    return (2u << 4)                      // D format s32
+           | (0u << 7) | (0u << 10)       // A, B unsigned 8-bit
+           | ((uint32_t)(N >> 3) << 17)   // N / 8
+           | ((uint32_t)(128 >> 4) << 24);  // M / 16
+}
+
+LDK_DEV void mma_u8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
+}
+LDK_DEV void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar))
+                 : "memory");
+}
+
+// 16 consecutive 32-bit TMEM columns of this warp's lane quarter; the wait takes the
+// registers as operands so no use can be scheduled before the load completes.
+LDK_DEV void tmem_ld16_wait(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+template <int P>
+LDK_DEV void tmem_wait_regs(uint32_t (&r)[P][16]) {
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        asm volatile("tcgen05.wait::ld.sync.aligned;"
+                     : "+r"(r[p][0]), "+r"(r[p][1]), "+r"(r[p][2]), "+r"(r[p][3]), "+r"(r[p][4]), "+r"(r[p][5]),
+                       "+r"(r[p][6]), "+r"(r[p][7]), "+r"(r[p][8]), "+r"(r[p][9]), "+r"(r[p][10]), "+r"(r[p][11]),
+                       "+r"(r[p][12]), "+r"(r[p][13]), "+r"(r[p][14]), "+r"(r[p][15])
+                     :
+                     : "memory");
+    }
+}
+
+LDK_DEV void epi_bar() { asm volatile("bar.sync 1, %0;" ::"n"(32 * kEpiWarps) : "memory"); }
+LDK_DEV bool epi_bar_or(bool pred) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "barrier.red.or.pred q, 1, %2, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "n"(32 * kEpiWarps)
+        : "memory");
+    return r != 0;
+}
+
+LDK_DEV void spin_ns(uint64_t ns) {
+    const uint64_t t0 = global_ns();
+    while (global_ns() - t0 < ns) {
+    }
+}
+
+// ---------------------------------------------------------------------------
+// indicator planes: planes[v][0][k] = [x == 1], planes[v][1][k] = [x in {0, 1}]
+// ---------------------------------------------------------------------------
+
+struct PrepArgs {
+    const int8_t* X;
+    int64_t ld;
+    int64_t n_var;
+    const int32_t* pop_rows;
+    int pop_off[LDK_MAX_POPS + 1];
+    int kofs[LDK_MAX_POPS + 1];
+    int P;
+    int ktot;
+    uint8_t* planes;
+    unsigned* status;
+};
+
+constexpr int kPrepV = 64, kPrepK = 128;
+
+__global__ void __launch_bounds__(256) k_prep_planes(PrepArgs a) {
+    __shared__ int8_t tile[kPrepK][kPrepV + 4];
+    const int64_t v0 = (int64_t)blockIdx.x * kPrepV;
+    const int k0 = blockIdx.y * kPrepK;
+    // gather: tile[k][v] = X[row(k), v0 + v] (coalesced along v); 127 marks padding
+    for (int idx = threadIdx.x; idx < kPrepK * kPrepV; idx += blockDim.x) {
+        const int kk = idx / kPrepV, vv = idx % kPrepV;
+        const int k = k0 + kk;
+        const int64_t v = v0 + vv;
+        int8_t x = 127;
+        if (v < a.n_var) {
+            int p = 0;
+            while (p + 1 < a.P && k >= a.kofs[p + 1]) ++p;
+            const int local = k - a.kofs[p];
+            const int np = a.pop_off[p + 1] - a.pop_off[p];
+            if (local >= 0 && local < np && k < a.kofs[a.P]) {
+                const int row = a.pop_rows[a.pop_off[p] + local];
+                x = a.X[(int64_t)row * a.ld + v];
+                if (x < -1 || x > 1) atomicOr(a.status, LDK_DEVERR_BAD_INPUT);
+            }
+        }
+        tile[kk][vv] = x;
+    }
+    __syncthreads();
+    // scatter: 4 bytes of one plane per thread, coalesced along k
+    for (int idx = threadIdx.x; idx < kPrepV * 2 * (kPrepK / 4); idx += blockDim.x) {
+        const int kq = idx % (kPrepK / 4);
+        const int plane = (idx / (kPrepK / 4)) % 2;
+        const int vv = idx / (2 * (kPrepK / 4));
+        const int64_t v = v0 + vv;
+        if (v >= a.n_var) continue;
+        uint32_t w = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int8_t x = tile[4 * kq + b][vv];
+            const uint32_t bit = plane == 0 ? (x == 1) : (x == 0 || x == 1);
+            w |= bit << (8 * b);
+        }
+        *reinterpret_cast<uint32_t*>(a.planes + (v * 2 + plane) * (int64_t)a.ktot + k0 + 4 * kq) = w;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// the fused count + estimator + bin kernel
+// ---------------------------------------------------------------------------
+
+struct TcArgs {
+    const double* coord;
+    const int32_t* jmax;
+    const int32_t* snp_block;
+    int n_blocks;
+    const int32_t* items;  // (n_items, 2): [row0, row1) row blocks
+    int n_items;
+    int nkc;               // K chunks of 128 bytes
+    int kofs[LDK_MAX_POPS + 1];
+    BinEdges edges;
+    double* sums;
+    double* r2_sums;
+    unsigned long long* pairs;
+    unsigned long long* r2_counts;
+    unsigned* status;
+};
+
+template <int P>
+__global__ void __launch_bounds__(kThreadsTC, 1)
+    k_parse_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcArgs a) {
+    using C = Cfg<P>;
+    constexpr int NS = C::NS;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int nb = a.edges.n_bins;
+    unsigned char* stages = base;
+    double* sacc = reinterpret_cast<double*>(base + C::STAGES * C::STAGE_BYTES);      // [kSlots][nb][NS+1]
+    unsigned* scnt = reinterpret_cast<unsigned*>(sacc + kSlots * nb * (NS + 1));        // [kSlots][nb][2]
+
+    __shared__ __align__(8) uint64_t full_bar[C::STAGES], empty_bar[C::STAGES], tfull[2], tempty[2];
+    __shared__ uint32_t tmem_base_s;
+    __shared__ volatile int abort_s;
+    __shared__ double sedges[LDK_MAX_BINS + 1];
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < C::STAGES; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], kEpiWarps);
+        }
+        abort_s = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int b = threadIdx.x; b <= nb; b += blockDim.x) sedges[b] = a.edges.e[b];
+    for (int idx = threadIdx.x; idx < kSlots * nb * (NS + 1); idx += blockDim.x) sacc[idx] = 0.0;
+    for (int idx = threadIdx.x; idx < kSlots * nb * 2; idx += blockDim.x) scnt[idx] = 0u;
+    if (warp == 1) {
+        tmem_alloc(&tmem_base_s, kTmemCols);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base_s;
+
+    if (warp == 0) {
+        // ------------------------------------------------------------- TMA producer
+        if (lane == 0) {
+            uint32_t it = 0;
+            bool ok = true;
+            for (int item = blockIdx.x; item < a.n_items && ok; item += gridDim.x) {
+                const int row0 = a.items[2 * item], row1 = a.items[2 * item + 1];
+                const int jend = a.jmax[row1 - 1];
+                const int n_jt = jend > row0 + 1 ? (jend - row0 + C::NJ - 1) / C::NJ : 0;
+                for (int t = 0; t < n_jt && ok; ++t) {
+                    const int j0 = row0 + t * C::NJ;
+                    for (int c = 0; c < a.nkc; ++c, ++it) {
+                        const int s = it % C::STAGES;
+                        const uint32_t ph = (it / C::STAGES) & 1u;
+                        if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_s, a.status)) { ok = false; break; }
+                        unsigned char* dst = stages + s * C::STAGE_BYTES;
+                        mbar_expect_tx(&full_bar[s], C::STAGE_BYTES);
+                        tma_load_3d(dst, &tmA, &full_bar[s], c * kKChunk, 0, row0);
+                        tma_load_3d(dst + C::A_BYTES, &tmB, &full_bar[s], c * kKChunk, 0, j0);
+                    }
+                }
+            }
+            if (!ok) spin_ns(2000000);  // let copies already issued land before teardown
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        // ------------------------------------------------------------- MMA issuer
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_u8<C::N>();
+            uint32_t it = 0, tcount = 0;
+            bool ok = true;
+            for (int item = blockIdx.x; item < a.n_items && ok; item += gridDim.x) {
+                const int row0 = a.items[2 * item], row1 = a.items[2 * item + 1];
+                const int jend = a.jmax[row1 - 1];
+                const int n_jt = jend > row0 + 1 ? (jend - row0 + C::NJ - 1) / C::NJ : 0;
+                for (int t = 0; t < n_jt && ok; ++t, ++tcount) {
+                    const uint32_t buf = tcount & 1u, tph = (tcount >> 1) & 1u;
+                    if (!mbar_wait(&tempty[buf], tph ^ 1u, &abort_s, a.status)) { ok = false; break; }
+                    tc_fence_after();
+                    for (int c = 0; c < a.nkc; ++c, ++it) {
+                        const int s = it % C::STAGES;
+                        const uint32_t ph = (it / C::STAGES) & 1u;
+                        if (!mbar_wait(&full_bar[s], ph, &abort_s, a.status)) { ok = false; break; }
+                        tc_fence_after();
+                        const uint32_t a_addr = su32(stages + s * C::STAGE_BYTES);
+                        const uint32_t b_addr = a_addr + C::A_BYTES;
+#pragma unroll
+                        for (int ks = 0; ks < kKChunk / 32; ++ks) {
+                            const int kbyte = c * kKChunk + ks * 32;
+                            int p = 0;
+#pragma unroll
+                            for (int q = 1; q < P; ++q) p += (kbyte >= a.kofs[q]) ? 1 : 0;
+                            const uint32_t first = (kbyte == a.kofs[p]) ? 1u : 0u;
+                            const uint32_t d = tmem + buf * C::COLS + p * C::N;
+                            mma_u8(d, sw128_desc(a_addr + ks * 32), sw128_desc(b_addr + ks * 32), idesc, first ^ 1u);
+                        }
+                        mma_commit(&empty_bar[s]);
+                    }
+                    if (!ok) break;
+                    mma_commit(&tfull[buf]);
+                }
+            }
+            if (!ok) spin_ns(2000000);
+        }
+        __syncwarp();
+    } else {
+        // ------------------------------------------------------------- epilogue
+        const int e = warp - 2;
+        const int quarter = warp & 3, half = e >> 2;
+        const int L = quarter * 32 + lane;
+        const int r = L >> 1, role = L & 1;
+        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+        constexpr int CH = C::NJ / 16;  // chunks of 8 partners per half
+        uint32_t tcount = 0;
+        for (int item = blockIdx.x; item < a.n_items; item += gridDim.x) {
+            if (epi_bar_or(abort_s != 0)) break;
+            const int row0 = a.items[2 * item], row1 = a.items[2 * item + 1];
+            const int jend = a.jmax[row1 - 1];
+            const int n_jt = jend > row0 + 1 ? (jend - row0 + C::NJ - 1) / C::NJ : 0;
+            if (n_jt == 0) continue;
+            const int i = row0 + r;
+            bool row_ok = i < row1;
+            const int my_jmax = row_ok ? a.jmax[i] : 0;
+            const double ci = row_ok ? a.coord[i] : 0.0;
+            const int blk0 = a.snp_block ? a.snp_block[row0] : 0;
+            int slot = 0;
+            if (row_ok && a.snp_block) {
+                slot = a.snp_block[i] - blk0;
+                if (slot < 0 || slot >= kSlots) {
+                    atomicOr(a.status, LDK_DEVERR_BLOCK_SPAN);
+                    row_ok = false;
+                }
+            }
+            float acc[NS];
+#pragma unroll
+            for (int s = 0; s < NS; ++s) acc[s] = 0.f;
+            float r2acc = 0.f;
+            unsigned np = 0, nr2 = 0;
+            int cur = -1;
+            auto flush = [&]() {
+                if (cur >= 0 && cur < nb && np > 0) {
+                    double* dst = sacc + (slot * nb + cur) * (NS + 1);
+#pragma unroll
+                    for (int s = 0; s < NS; ++s) atomicAdd(dst + s, (double)acc[s]);
+                    atomicAdd(dst + NS, (double)r2acc);
+                    atomicAdd(scnt + 2 * (slot * nb + cur), np);
+                    atomicAdd(scnt + 2 * (slot * nb + cur) + 1, nr2);
+                }
+#pragma unroll
+                for (int s = 0; s < NS; ++s) acc[s] = 0.f;
+                r2acc = 0.f;
+                np = nr2 = 0;
+            };
+            bool ok = true;
+            for (int t = 0; t < n_jt; ++t, ++tcount) {
+                const uint32_t buf = tcount & 1u, tph = (tcount >> 1) & 1u;
+                if (!mbar_wait(&tfull[buf], tph, &abort_s, a.status)) { ok = false; break; }
+                tc_fence_after();
+                const int j0 = row0 + t * C::NJ;
+#pragma unroll 1
+                for (int ch = 0; ch < CH; ++ch) {
+                    uint32_t v[P][16];
+                    const uint32_t col = buf * C::COLS + half * C::NJ + ch * 16;
+#pragma unroll
+                    for (int p = 0; p < P; ++p) tmem_ld16_wait(tmem + lane_base + col + p * C::N, v[p]);
+                    tmem_wait_regs<P>(v);
+                    if (ch == CH - 1) {
+                        tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(&tempty[buf]);
+                    }
+#pragma unroll
+                    for (int tt = 0; tt < 4; ++tt) {
+                        HapFeat<float> f[P];
+#pragma unroll
+                        for (int p = 0; p < P; ++p) {
+                            // lane 2r: (hh, hv) of partners 2tt, 2tt+1; lane 2r+1: (vh, vv)
+                            const uint32_t sx = role ? v[p][4 * tt + 0] : v[p][4 * tt + 2];
+                            const uint32_t sy = role ? v[p][4 * tt + 1] : v[p][4 * tt + 3];
+                            const uint32_t rx = __shfl_xor_sync(0xffffffffu, sx, 1);
+                            const uint32_t ry = __shfl_xor_sync(0xffffffffu, sy, 1);
+                            int hh, hv, vh, vv;
+                            if (role == 0) { hh = (int)v[p][4 * tt]; hv = (int)v[p][4 * tt + 1]; vh = (int)rx; vv = (int)ry; }
+                            else { vh = (int)v[p][4 * tt + 2]; vv = (int)v[p][4 * tt + 3]; hh = (int)rx; hv = (int)ry; }
+                            hap_set_counts(f[p], float(hh), float(hv - hh), float(vh - hh), float(vv - hv - vh + hh));
+                        }
+                        const int jj = half * (C::NJ / 2) + ch * 8 + 2 * tt + role;
+                        const int j = j0 + jj;
+                        if (row_ok && j > i && j < my_jmax) {
+                            const int b = bin_advance(sedges, nb, cur, fabs(a.coord[j] - ci));
+                            if (b != cur) {
+                                flush();
+                                cur = b;
+                            }
+                            if (b >= 0 && b < nb) {
+#pragma unroll
+                                for (int p = 0; p < P; ++p) hap_features<float, P>(f[p]);
+                                hap_stats<float, P>(f, acc);
+                                float r2;
+                                if (hap_r2(f[0], r2)) { r2acc += r2; ++nr2; }
+                                ++np;
+                            }
+                        }
+                    }
+                }
+            }
+            flush();
+            (void)ok;
+            // stage -> global, once per row block
+            epi_bar();
+            const int et = threadIdx.x - 64;
+            for (int idx = et; idx < kSlots * nb * (NS + 1); idx += 32 * kEpiWarps) {
+                const int sl = idx / (nb * (NS + 1));
+                const int rem = idx % (nb * (NS + 1));
+                const int bb = rem / (NS + 1), s = rem % (NS + 1);
+                const double val = sacc[idx];
+                const int blk = blk0 + sl;
+                if (val != 0.0 && blk < a.n_blocks) {
+                    if (s < NS) atomicAdd(&a.sums[((int64_t)blk * nb + bb) * NS + s], val);
+                    else atomicAdd(&a.r2_sums[(int64_t)blk * nb + bb], val);
+                }
+                sacc[idx] = 0.0;
+            }
+            for (int idx = et; idx < kSlots * nb; idx += 32 * kEpiWarps) {
+                const int blk = blk0 + idx / nb, bb = idx % nb;
+                if (blk < a.n_blocks) {
+                    if (scnt[2 * idx]) atomicAdd(&a.pairs[(int64_t)blk * nb + bb], (unsigned long long)scnt[2 * idx]);
+                    if (scnt[2 * idx + 1])
+                        atomicAdd(&a.r2_counts[(int64_t)blk * nb + bb], (unsigned long long)scnt[2 * idx + 1]);
+                }
+                scnt[2 * idx] = 0u;
+                scnt[2 * idx + 1] = 0u;
+            }
+            epi_bar();
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem, kTmemCols);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+bool make_map(CUtensorMap* m, const uint8_t* planes, int64_t n_var, int ktot, int rows_box) {
+    auto fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)ktot, 2, (cuuint64_t)n_var};
+    cuuint64_t strides[2] = {(cuuint64_t)ktot, (cuuint64_t)ktot * 2};
+    cuuint32_t box[3] = {(cuuint32_t)kKChunk, 2, (cuuint32_t)rows_box};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<uint8_t*>(planes), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+template <int P>
+size_t smem_bytes_t(int nb) {
+    using C = Cfg<P>;
+    return 1024 + (size_t)C::STAGES * C::STAGE_BYTES + (size_t)kSlots * nb * (C::NS + 1) * sizeof(double) +
+           (size_t)kSlots * nb * 2 * sizeof(unsigned);
+}
+
+}  // namespace
+
+int tc_rows_per_block(const ParseShape&) { return kRows; }
+
+size_t tc_smem_bytes(const ParseShape& sh) {
+    switch (sh.P) {
+        case 1: return smem_bytes_t<1>(sh.n_bins);
+        case 2: return smem_bytes_t<2>(sh.n_bins);
+        case 3: return smem_bytes_t<3>(sh.n_bins);
+        default: return smem_bytes_t<4>(sh.n_bins);
+    }
+}
+
+cudaError_t launch_prep_planes(const ldk_parse_t* d, const Scratch& w, const ParseShape& sh, cudaStream_t s) {
+    if (d->n_var == 0) return cudaSuccess;
+    PrepArgs a;
+    a.X = d->X;
+    a.ld = d->ld_x;
+    a.n_var = d->n_var;
+    a.pop_rows = d->pop_rows;
+    for (int p = 0; p <= LDK_MAX_POPS; ++p) {
+        a.pop_off[p] = d->pop_offsets[p];
+        a.kofs[p] = sh.kofs[p];
+    }
+    a.P = sh.P;
+    a.ktot = sh.ktot;
+    a.planes = w.hv;
+    a.status = w.status;
+    dim3 grid((unsigned)((d->n_var + kPrepV - 1) / kPrepV), (unsigned)(sh.ktot / kPrepK));
+    k_prep_planes<<<grid, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int P>
+static cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w,
+                                     const ParseShape& sh, int n_items, cudaStream_t s) {
+    using C = Cfg<P>;
+    CUtensorMap mA, mB;
+    if (!make_map(&mA, w.hv, d->n_var, sh.ktot, kRows) || !make_map(&mB, w.hv, d->n_var, sh.ktot, C::NJ))
+        return cudaErrorInvalidValue;
+    TcArgs a;
+    a.coord = d->coord ? d->coord : d->pos;
+    a.jmax = w.jmax;
+    a.snp_block = d->snp_block;
+    a.n_blocks = d->n_blocks;
+    a.items = w.items;
+    a.n_items = n_items;
+    a.nkc = sh.ktot / kKChunk;
+    for (int p = 0; p <= LDK_MAX_POPS; ++p) a.kofs[p] = sh.kofs[p];
+    a.edges.n_bins = d->n_bins;
+    for (int b = 0; b <= LDK_MAX_BINS; ++b) a.edges.e[b] = b <= d->n_bins ? d->edges[b] : 0.0;
+    a.sums = o->sums;
+    a.r2_sums = o->r2_sums;
+    a.pairs = reinterpret_cast<unsigned long long*>(o->pairs);
+    a.r2_counts = reinterpret_cast<unsigned long long*>(o->r2_counts);
+    a.status = w.status;
+    const size_t smem = smem_bytes_t<P>(d->n_bins);
+    cudaError_t e = cudaFuncSetAttribute(k_parse_tc<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (n_items == 0) return cudaSuccess;
+    const int grid = n_items < sms ? n_items : sms;
+    k_parse_tc<P><<<grid, kThreadsTC, smem, s>>>(mA, mB, a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_parse_tc(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w,
+                            const ParseShape& sh, int n_items, cudaStream_t s) {
+    switch (sh.P) {
+        case 1: return launch_parse_tc_p<1>(d, o, w, sh, n_items, s);
+        case 2: return launch_parse_tc_p<2>(d, o, w, sh, n_items, s);
+        case 3: return launch_parse_tc_p<3>(d, o, w, sh, n_items, s);
+        case 4: return launch_parse_tc_p<4>(d, o, w, sh, n_items, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace ldk

@@ -1,0 +1,269 @@
+"""GPU parity: libldk (through its C ABI) against the float64 oracle and the reference's
+golden vectors.  Tolerances: counts and pair tallies bit-exact; plain FP64 path 1e-12
+relative (1e-15 absolute) per value / per bin; tensor-core path (FP32 estimators, FP64
+bin sums) 1e-6 relative per bin."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from oracle import ld_oracle as O
+from pg_gpu_b200 import _lib, parse, synth
+from pg_gpu_b200.csrc import gen_estimators as G
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+PLAIN_RTOL = 1e-12
+TC_RTOL = 1e-6
+
+
+def rel_err(got, want, floor):
+    got, want = np.asarray(got, np.float64), np.asarray(want, np.float64)
+    d = np.abs(got - want)
+    scale = np.maximum(np.abs(want), floor)
+    return float(np.max(d / scale)) if d.size else 0.0
+
+
+def dev(a, dtype):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device="cuda")
+
+
+@pytest.fixture(scope="module")
+def ref_hap(golden_dir):
+    return np.load(os.path.join(golden_dir, "ref_hap.npz"))
+
+
+@pytest.fixture(scope="module")
+def ref_geno(golden_dir):
+    return np.load(os.path.join(golden_dir, "ref_geno.npz"))
+
+
+def _stream():
+    return _lib.stream_handle()
+
+
+@pytest.mark.parametrize("P", [1, 2, 3, 4])
+def test_counts_hap_bit_exact(ref_hap, P):
+    lib = _lib.load()
+    g = ref_hap
+    hap, offs = g[f"P{P}_hap"], g[f"P{P}_offs"]
+    ii, jj = g[f"P{P}_ii"], g[f"P{P}_jj"]
+    X, I, J = dev(hap, torch.int8), dev(ii, torch.int32), dev(jj, torch.int32)
+    n = len(ii)
+    for q in range(P):
+        rows = dev(np.arange(offs[q], offs[q + 1]), torch.int32)
+        counts = torch.empty((n, 4), dtype=torch.int32, device="cuda")
+        nv = torch.empty(n, dtype=torch.int32, device="cuda")
+        _lib.check(lib.ldk_counts_hap(_lib.ptr(X), hap.shape[1], hap.shape[1], _lib.ptr(rows), rows.numel(),
+                                      _lib.ptr(I), _lib.ptr(J), n, _lib.ptr(counts), _lib.ptr(nv), _stream()))
+        np.testing.assert_array_equal(counts.cpu().numpy(), g[f"P{P}_counts{q}"])
+        ref_nv = g[f"P{P}_nvalid{q}"]
+        if (ref_nv >= 0).all():
+            np.testing.assert_array_equal(nv.cpu().numpy(), ref_nv)
+
+
+@pytest.mark.parametrize("P", [1, 2, 3, 4])
+def test_counts_geno_bit_exact(ref_geno, P):
+    lib = _lib.load()
+    g = ref_geno
+    geno, offs = g[f"P{P}_geno"], g[f"P{P}_offs"]
+    ii, jj = g[f"P{P}_ii"], g[f"P{P}_jj"]
+    X, I, J = dev(geno, torch.int8), dev(ii, torch.int32), dev(jj, torch.int32)
+    n = len(ii)
+    for q in range(P):
+        rows = dev(np.arange(offs[q], offs[q + 1]), torch.int32)
+        counts = torch.empty((n, 9), dtype=torch.int32, device="cuda")
+        nv = torch.empty(n, dtype=torch.int32, device="cuda")
+        _lib.check(lib.ldk_counts_geno(_lib.ptr(X), geno.shape[1], geno.shape[1], _lib.ptr(rows), rows.numel(),
+                                       _lib.ptr(I), _lib.ptr(J), n, _lib.ptr(counts), _lib.ptr(nv), _stream()))
+        np.testing.assert_array_equal(counts.cpu().numpy(), g[f"P{P}_counts{q}"])
+
+
+def _stats(genotypes, counts_list, nvalid_list):
+    lib = _lib.load()
+    P = len(counts_list)
+    n = counts_list[0].shape[0]
+    C = dev(np.stack(counts_list), torch.int32)
+    NV = None
+    if any(v is not None for v in nvalid_list):
+        NV = dev(np.stack([v if v is not None else c.sum(axis=1) for v, c in zip(nvalid_list, counts_list)]),
+                 torch.int32)
+    out = torch.empty((n, parse.n_stats(P)), dtype=torch.float64, device="cuda")
+    _lib.check(lib.ldk_stats(int(genotypes), P, _lib.ptr(C), _lib.ptr(NV), n, _lib.ptr(out), _stream()))
+    return out.cpu().numpy()
+
+
+@pytest.mark.parametrize("P", [1, 2, 3, 4])
+def test_stats_hap_golden(ref_hap, P):
+    g = ref_hap
+    cl = [g[f"P{P}_counts{q}"] for q in range(P)]
+    nl = [None if (g[f"P{P}_nvalid{q}"] < 0).all() else g[f"P{P}_nvalid{q}"] for q in range(P)]
+    got = _stats(False, cl, nl)
+    assert rel_err(got, g[f"P{P}_stats"], 1e-3) < PLAIN_RTOL
+    if P == 2:
+        assert rel_err(got, g["P2_twopop_stats"], 1e-3) < PLAIN_RTOL
+
+
+@pytest.mark.parametrize("P", [1, 2, 3, 4])
+def test_stats_geno_golden(ref_geno, P):
+    g = ref_geno
+    cl = [g[f"P{P}_counts{q}"] for q in range(P)]
+    nl = [None if (g[f"P{P}_nvalid{q}"] < 0).all() else g[f"P{P}_nvalid{q}"] for q in range(P)]
+    got = _stats(True, cl, nl)
+    ref = g[f"P{P}_stats"]
+    assert np.array_equal(np.isfinite(got), np.isfinite(ref))
+    f = np.isfinite(ref)
+    assert rel_err(got[f], ref[f], 1e-3) < PLAIN_RTOL
+
+
+def test_raw_calls_every_case():
+    """ldk_raw_hap for every canonical case against the oracle's raw call."""
+    lib = _lib.load()
+    rng = np.random.default_rng(7)
+    P = 4
+    n = 500
+    counts = [rng.multinomial(rng.integers(3, 60), [0.3, 0.2, 0.2, 0.3], size=n) for _ in range(P)]
+    for c in counts:
+        c[:5] = [[0, 0, 0, 3], [1, 0, 0, 0], [0, 0, 0, 0], [2, 0, 0, 2], [0, 1, 1, 0]]
+    pops = [O.HapPop(c) for c in counts]
+    C = dev(np.concatenate(counts, axis=1).astype(np.float64), torch.float64)
+    examples = {"dd1": ("dd", (1, 1)), "dd2": ("dd", (0, 2)), "dz_iii": ("dz", (2, 2, 2)),
+                "dz_iij": ("dz", (1, 1, 3)), "dz_iji": ("dz", (0, 2, 0)), "dz_ijj": ("dz", (3, 1, 1)),
+                "dz_ijk": ("dz", (0, 1, 2)), "pi2_same": ("pi2", (3, 3, 3, 3)),
+                "pi2_iikk": ("pi2", (0, 0, 2, 2)), "pi2_iikl": ("pi2", (1, 1, 0, 3)),
+                "pi2_ijkk": ("pi2", (0, 2, 3, 3)), "pi2_alldiff": ("pi2", (0, 1, 2, 3)),
+                "pi2_triple": ("pi2", (2, 1, 2, 2)), "pi2_ijij": ("pi2", (1, 3, 1, 3)),
+                "pi2_shared": ("pi2", (0, 1, 0, 2))}
+    for cid, case in enumerate(G.RAW_CASES):
+        kind, q = examples[case]
+        ccase, args = G.canonical(kind, q)
+        assert ccase == case
+        a = (ctypes.c_int32 * 4)(*(list(args) + [0] * (4 - len(args))))
+        out = torch.empty(n, dtype=torch.float64, device="cuda")
+        _lib.check(lib.ldk_raw_hap(cid, a, P, _lib.ptr(C), None, n, _lib.ptr(out), _stream()))
+        want = O.hap_raw(kind, q, pops)
+        assert rel_err(out.cpu().numpy(), want, 1e-3) < PLAIN_RTOL, case
+
+
+def test_r_family_golden(ref_hap):
+    lib = _lib.load()
+    g = ref_hap
+    hap, offs, ii, jj = g["P1_hap"], g["P1_offs"], g["P1_ii"], g["P1_jj"]
+    c, nv = O.hap_counts(hap, ii, jj, list(range(offs[0], offs[1])))
+    C = dev(c.astype(np.float64), torch.float64)
+    for which, key in ((0, "P1_r"), (1, "P1_r2"), (2, "P1_dprime")):
+        out = torch.empty(len(c), dtype=torch.float64, device="cuda")
+        _lib.check(lib.ldk_r_family(which, _lib.ptr(C), None, len(c), _lib.ptr(out), _stream()))
+        np.testing.assert_allclose(out.cpu().numpy(), g[key], rtol=1e-12, atol=1e-15, equal_nan=True)
+    e = g["edge_counts"]
+    out = torch.empty(len(e), dtype=torch.float64, device="cuda")
+    _lib.check(lib.ldk_r_family(1, _lib.ptr(dev(e, torch.float64)), None, len(e), _lib.ptr(out), _stream()))
+    np.testing.assert_allclose(out.cpu().numpy(), g["edge_r2"], rtol=1e-12, equal_nan=True)
+
+
+# ---------------------------------------------------------------------------
+# the binned parse
+# ---------------------------------------------------------------------------
+
+SCALES = {1: 0.1, 2: 0.004, 3: 0.003, 4: 0.004, 5: 0.0015}
+
+
+@pytest.fixture(scope="module")
+def workloads():
+    return {k: synth.make_config(k, scale=s) for k, s in SCALES.items()}
+
+
+@pytest.fixture(scope="module")
+def oracle_results(workloads):
+    out = {}
+    for k, w in workloads.items():
+        out[k] = O.bin_sums(w.data, w.positions, w.pop_rows, w.edges, genotypes=w.genotypes,
+                            max_dist=w.max_dist, window_offsets=w.window_offsets, snp_block=w.snp_block,
+                            n_blocks=w.n_blocks)
+    return out
+
+
+def run_parse(w, method):
+    r = parse.ld_parse(w.data, w.positions, w.pop_rows, w.edges, genotypes=w.genotypes, method=method,
+                       max_dist=w.max_dist, window_offsets=w.window_offsets, snp_block=w.snp_block,
+                       n_blocks=w.n_blocks)
+    return r.numpy()
+
+
+def check_parse(got, want, rtol):
+    np.testing.assert_array_equal(got["pairs"], want["pairs"])
+    np.testing.assert_array_equal(got["r2_counts"], want["r2_count"])
+    assert want["pairs"].sum() > 0
+    # per-bin relative error against the FP64 oracle, scaled by the bin's magnitude
+    floor = 1e-300
+    assert rel_err(got["sums"], want["sums"], floor) < rtol
+    assert rel_err(got["r2_sums"], want["r2_sum"], floor) < rtol
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 4, 5])
+def test_parse_plain_matches_oracle(workloads, oracle_results, k):
+    check_parse(run_parse(workloads[k], "plain"), oracle_results[k], PLAIN_RTOL)
+
+
+@pytest.mark.parametrize("k", [1, 2, 4, 5])
+def test_parse_tc_matches_oracle(workloads, oracle_results, k):
+    check_parse(run_parse(workloads[k], "tc"), oracle_results[k], TC_RTOL)
+
+
+def test_im_example_against_moments(golden_dir):
+    im = np.load(os.path.join(golden_dir, "im_example.npz"))
+    hap, pos = im["hap"], im["pos"].astype(np.float64)
+    keep = O.biallelic_keep(hap)
+    hap, pos = hap[:, keep], pos[keep]
+    rows = [im["rows0"], im["rows1"]]
+    for method, tol in (("plain", 1e-10), ("tc", TC_RTOL)):
+        r = parse.ld_parse(hap, pos, rows, im["edges"], method=method).numpy()
+        assert rel_err(r["sums"][0], im["ld_sums"], 1e-300) < tol, method
+
+
+def test_parse_edge_cases():
+    rng = np.random.default_rng(3)
+    hap = rng.integers(0, 2, size=(12, 40)).astype(np.int8)
+    pos = np.arange(40, dtype=np.float64) * 10.0
+    rows = [np.arange(12)]
+    for method in ("plain", "tc"):
+        # max_dist 0 with unique positions: no pairs
+        r = parse.ld_parse(hap, pos, rows, [0.0, 5.0], method=method, max_dist=0.0).numpy()
+        assert r["pairs"].sum() == 0 and np.all(r["sums"] == 0)
+        # a single SNP: nothing to do
+        r = parse.ld_parse(hap[:, :1], pos[:1], rows, [0.0, 5.0], method=method).numpy()
+        assert r["pairs"].sum() == 0
+        # distance exactly on the last edge is generated but dropped; below the first edge dropped
+        r = parse.ld_parse(hap, pos, rows, [15.0, 30.0], method=method).numpy()
+        want = O.bin_sums(hap, pos, rows, [15.0, 30.0])
+        np.testing.assert_array_equal(r["pairs"], want["pairs"])
+        assert want["n_pairs"] > want["pairs"].sum()
+        # empty and one-SNP windows
+        wo = np.array([0, 0, 1, 17, 17, 40])
+        r = parse.ld_parse(hap, pos, rows, [0.0, 100.0, 1000.0], method=method, window_offsets=wo).numpy()
+        want = O.bin_sums(hap, pos, rows, [0.0, 100.0, 1000.0], window_offsets=wo)
+        np.testing.assert_array_equal(r["pairs"], want["pairs"])
+        assert rel_err(r["sums"], want["sums"], 1e-300) < (PLAIN_RTOL if method == "plain" else TC_RTOL)
+
+
+def test_parse_reports_errors():
+    hap = np.zeros((4, 10), np.int8)
+    hap[0] = 1
+    pos = np.arange(10, dtype=np.float64)
+    with pytest.raises(_lib.LdkError, match="unsorted"):
+        parse.ld_parse(hap, pos[::-1].copy(), [np.arange(4)], [0.0, 5.0], method="plain")
+    with pytest.raises(_lib.LdkError, match="snp_block"):
+        parse.ld_parse(hap, pos, [np.arange(4)], [0.0, 5.0], method="plain",
+                       snp_block=np.full(10, 3, np.int32), n_blocks=2)
+    with pytest.raises(_lib.LdkError, match="edges"):
+        parse.ld_parse(hap, pos, [np.arange(4)], [5.0, 1.0], method="plain")
+
+
+def test_block_combine_bootstrap():
+    rng = np.random.default_rng(11)
+    bs = rng.normal(size=(30, 4, 15))
+    w = rng.integers(0, 3, size=(7, 30)).astype(np.int32)
+    got = parse.block_combine(dev(bs, torch.float64), w).cpu().numpy()
+    np.testing.assert_allclose(got, np.tensordot(w, bs, axes=(1, 0)), rtol=1e-13, atol=1e-13)
