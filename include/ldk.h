@@ -40,7 +40,8 @@ extern "C" {
 
 /* counting / estimator method of ldk_parse */
 #define LDK_METHOD_PLAIN_FP64 0 /* per-pair byte counting + FP64 estimators (the drop-in) */
-#define LDK_METHOD_TC 1         /* INT8 tcgen05 Gram counts + FP32 estimators, FP64 bins */
+#define LDK_METHOD_TC 1         /* INT8 tcgen05 Gram counts; exact-integer features, FP64 combination and bins */
+#define LDK_METHOD_TC_FP32 2    /* INT8 tcgen05 Gram counts; FP32 estimators, FP64 bins (error ~1e-7 of a bin's absolute mass) */
 
 LDK_API int ldk_version(void);
 LDK_API const char* ldk_last_error(void);

@@ -78,7 +78,7 @@ Layout layout_of(const ldk_parse_t* d, const ParseShape& sh) {
     off = align_up(off + (size_t)d->n_var * sizeof(int32_t), 256);
     L.win_off = off;
     off = align_up(off + (size_t)(window_count(d) + 1) * sizeof(int64_t), 256);
-    if (d->method == LDK_METHOD_TC) {
+    if (d->method != LDK_METHOD_PLAIN_FP64) {
         int n_items = 0;
         for (int w = 0; w < window_count(d); ++w) {
             const int64_t m = window_bound(d, w + 1) - window_bound(d, w);
@@ -107,7 +107,10 @@ int validate(const ldk_parse_t* d) {
     for (int p = 0; p < d->n_pops; ++p)
         if (d->pop_offsets[p + 1] <= d->pop_offsets[p]) { set_error("empty population %d", p); return LDK_ERR_ARG; }
     if (d->n_blocks < 1) { set_error("n_blocks must be >= 1"); return LDK_ERR_ARG; }
-    if (d->method != LDK_METHOD_PLAIN_FP64 && d->method != LDK_METHOD_TC) { set_error("unknown method"); return LDK_ERR_ARG; }
+    if (d->method != LDK_METHOD_PLAIN_FP64 && d->method != LDK_METHOD_TC && d->method != LDK_METHOD_TC_FP32) {
+        set_error("unknown method");
+        return LDK_ERR_ARG;
+    }
     if (!(d->max_dist >= 0.0)) { set_error("max_dist must be >= 0"); return LDK_ERR_ARG; }
     if (d->window_offsets) {
         if (d->n_windows < 1) { set_error("n_windows must be >= 1"); return LDK_ERR_ARG; }
@@ -118,7 +121,7 @@ int validate(const ldk_parse_t* d) {
         for (int w = 0; w < d->n_windows; ++w)
             if (d->window_offsets[w + 1] < d->window_offsets[w]) { set_error("window_offsets must not decrease"); return LDK_ERR_ARG; }
     }
-    if (d->method == LDK_METHOD_TC && d->genotypes) {
+    if (d->method != LDK_METHOD_PLAIN_FP64 && d->genotypes) {
         set_error("the tensor-core method covers the haplotype path; use LDK_METHOD_PLAIN_FP64 for genotypes");
         return LDK_ERR_UNSUPPORTED;
     }
@@ -129,7 +132,7 @@ const char* status_text(unsigned s) {
     if (s & LDK_DEVERR_TIMEOUT) return "device wait timed out";
     if (s & LDK_DEVERR_BLOCK_RANGE) return "snp_block outside [0, n_blocks)";
     if (s & LDK_DEVERR_BLOCK_SPAN) return "a 64-SNP row block spans more than two bootstrap blocks";
-    if (s & LDK_DEVERR_BAD_INPUT) return "unsorted positions or allele codes outside {-1, 0, 1}";
+    if (s & LDK_DEVERR_BAD_INPUT) return "unsorted positions or coordinates, or allele codes outside {-1, 0, 1}";
     return "device error";
 }
 
@@ -230,7 +233,7 @@ int ldk_parse(const ldk_parse_t* d, const ldk_parse_out_t* out, void* workspace,
     }
     if (reinterpret_cast<uintptr_t>(workspace) % 256) { set_error("workspace must be 256-byte aligned"); return LDK_ERR_ARG; }
     if (int rc = check_arch()) return rc;
-    if (d->method == LDK_METHOD_TC && tc_smem_bytes(sh) > 227 * 1024) {
+    if (d->method != LDK_METHOD_PLAIN_FP64 && tc_smem_bytes(sh) > 227 * 1024) {
         set_error("bins x statistics exceed the tensor-core kernel's shared-memory staging");
         return LDK_ERR_UNSUPPORTED;
     }

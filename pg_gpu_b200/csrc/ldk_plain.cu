@@ -179,7 +179,7 @@ __global__ void k_r_family(int which, const double* __restrict__ counts, const d
 // pair ranges: jmax[i] = end of SNP i's partners (cutoff on pos, window end)
 // ---------------------------------------------------------------------------
 
-__global__ void k_jmax(const double* __restrict__ pos, int64_t n_var, const int64_t* __restrict__ win_off,
+__global__ void k_jmax(const double* __restrict__ pos, const double* __restrict__ coord, int64_t n_var, const int64_t* __restrict__ win_off,
                        int n_win, double max_dist, const int32_t* __restrict__ snp_block, int n_blocks,
                        int32_t* __restrict__ jmax, unsigned* __restrict__ status) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_var;
@@ -198,6 +198,7 @@ __global__ void k_jmax(const double* __restrict__ pos, int64_t n_var, const int6
         }
         jmax[i] = (int32_t)a;
         if (i + 1 < we && pos[i + 1] < pos[i]) atomicOr(status, LDK_DEVERR_BAD_INPUT);
+        if (coord && i + 1 < we && coord[i + 1] < coord[i]) atomicOr(status, LDK_DEVERR_BAD_INPUT);
         if (snp_block) {
             const int blk = snp_block[i];
             if (blk < 0 || blk >= n_blocks) atomicOr(status, LDK_DEVERR_BLOCK_RANGE);
@@ -469,7 +470,7 @@ cudaError_t launch_r_family(int which, const double* counts, const double* n_val
 
 cudaError_t launch_jmax(const ldk_parse_t* d, const Scratch& w, cudaStream_t s) {
     if (d->n_var == 0) return cudaSuccess;
-    k_jmax<<<blocks_for(d->n_var), kThreads, 0, s>>>(d->pos, d->n_var, w.win_off, d->n_windows, d->max_dist,
+    k_jmax<<<blocks_for(d->n_var), kThreads, 0, s>>>(d->pos, d->coord, d->n_var, w.win_off, d->n_windows, d->max_dist,
                                                       d->snp_block, d->n_blocks, w.jmax, w.status);
     return cudaGetLastError();
 }

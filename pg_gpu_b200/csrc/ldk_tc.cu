@@ -27,6 +27,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <cstdlib>
 #include <mutex>
 
 #include "ldk_estimators.cuh"
@@ -38,11 +39,12 @@ namespace {
 
 constexpr int kRows = 64;               // SNPs per row block (M = 128 = 64 x {h, v})
 constexpr int kKChunk = 128;            // K bytes per TMA box / swizzle row
-constexpr int kEpiWarps = 8;            // two per TMEM lane quarter
-constexpr int kThreadsTC = 64 + 32 * kEpiWarps;
+// epilogue warps: 4 (one per TMEM lane quarter, up to 255 registers) or 8 (two per
+// quarter, each covering half of the partner columns, up to 192 registers)
 constexpr int kSlots = 2;               // bootstrap blocks staged per row block
 constexpr int kTmemCols = 512;
 constexpr uint64_t kTimeoutNs = 5000000000ull;  // 5 s per wait
+constexpr size_t kMinSmem = 116 * 1024;
 
 template <int P>
 struct Cfg {
@@ -171,7 +173,9 @@ LDK_DEV void tmem_wait_regs(uint32_t (&r)[P][16]) {
     }
 }
 
-LDK_DEV void epi_bar() { asm volatile("bar.sync 1, %0;" ::"n"(32 * kEpiWarps) : "memory"); }
+template <int EPI>
+LDK_DEV void epi_bar() { asm volatile("bar.sync 1, %0;" ::"n"(32 * EPI) : "memory"); }
+template <int EPI>
 LDK_DEV bool epi_bar_or(bool pred) {
     uint32_t r;
     asm volatile(
@@ -180,7 +184,7 @@ LDK_DEV bool epi_bar_or(bool pred) {
         "barrier.red.or.pred q, 1, %2, p;\n\t"
         "selp.u32 %0, 1, 0, q;\n\t}"
         : "=r"(r)
-        : "r"((uint32_t)pred), "n"(32 * kEpiWarps)
+        : "r"((uint32_t)pred), "n"(32 * EPI)
         : "memory");
     return r != 0;
 }
@@ -273,8 +277,8 @@ struct TcArgs {
     unsigned* status;
 };
 
-template <int P>
-__global__ void __launch_bounds__(kThreadsTC, 1)
+template <int P, typename T, int EPI>
+__global__ void __maxnreg__(EPI == 8 ? 192 : 255)
     k_parse_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcArgs a) {
     using C = Cfg<P>;
     constexpr int NS = C::NS;
@@ -298,7 +302,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], kEpiWarps);
+            mbar_init(&tempty[b], EPI);
         }
         abort_s = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -382,15 +386,17 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
         __syncwarp();
     } else {
         // ------------------------------------------------------------- epilogue
+        constexpr int HALVES = EPI / 4;
+        constexpr int JPH = C::NJ / HALVES;  // partners per thread group
         const int e = warp - 2;
         const int quarter = warp & 3, half = e >> 2;
         const int L = quarter * 32 + lane;
         const int r = L >> 1, role = L & 1;
         const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
-        constexpr int CH = C::NJ / 16;  // chunks of 8 partners per half
+        constexpr int CH = JPH / 8;  // chunks of 8 partners
         uint32_t tcount = 0;
         for (int item = blockIdx.x; item < a.n_items; item += gridDim.x) {
-            if (epi_bar_or(abort_s != 0)) break;
+            if (epi_bar_or<EPI>(abort_s != 0)) break;
             const int row0 = a.items[2 * item], row1 = a.items[2 * item + 1];
             const int jend = a.jmax[row1 - 1];
             const int n_jt = jend > row0 + 1 ? (jend - row0 + C::NJ - 1) / C::NJ : 0;
@@ -408,10 +414,10 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
                     row_ok = false;
                 }
             }
-            float acc[NS];
+            T acc[NS];
 #pragma unroll
-            for (int s = 0; s < NS; ++s) acc[s] = 0.f;
-            float r2acc = 0.f;
+            for (int s = 0; s < NS; ++s) acc[s] = T(0);
+            T r2acc = T(0);
             unsigned np = 0, nr2 = 0;
             int cur = -1;
             auto flush = [&]() {
@@ -424,8 +430,8 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
                     atomicAdd(scnt + 2 * (slot * nb + cur) + 1, nr2);
                 }
 #pragma unroll
-                for (int s = 0; s < NS; ++s) acc[s] = 0.f;
-                r2acc = 0.f;
+                for (int s = 0; s < NS; ++s) acc[s] = T(0);
+                r2acc = T(0);
                 np = nr2 = 0;
             };
             bool ok = true;
@@ -437,7 +443,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
 #pragma unroll 1
                 for (int ch = 0; ch < CH; ++ch) {
                     uint32_t v[P][16];
-                    const uint32_t col = buf * C::COLS + half * C::NJ + ch * 16;
+                    const uint32_t col = buf * C::COLS + half * 2 * JPH + ch * 16;
 #pragma unroll
                     for (int p = 0; p < P; ++p) tmem_ld16_wait(tmem + lane_base + col + p * C::N, v[p]);
                     tmem_wait_regs<P>(v);
@@ -446,9 +452,9 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
                         __syncwarp();
                         if (lane == 0) mbar_arrive(&tempty[buf]);
                     }
-#pragma unroll
+#pragma unroll 1
                     for (int tt = 0; tt < 4; ++tt) {
-                        HapFeat<float> f[P];
+                        HapFeat<T> f[P];
 #pragma unroll
                         for (int p = 0; p < P; ++p) {
                             // lane 2r: (hh, hv) of partners 2tt, 2tt+1; lane 2r+1: (vh, vv)
@@ -459,9 +465,9 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
                             int hh, hv, vh, vv;
                             if (role == 0) { hh = (int)v[p][4 * tt]; hv = (int)v[p][4 * tt + 1]; vh = (int)rx; vv = (int)ry; }
                             else { vh = (int)v[p][4 * tt + 2]; vv = (int)v[p][4 * tt + 3]; hh = (int)rx; hv = (int)ry; }
-                            hap_set_counts(f[p], float(hh), float(hv - hh), float(vh - hh), float(vv - hv - vh + hh));
+                            hap_set_counts(f[p], T(hh), T(hv - hh), T(vh - hh), T(vv - hv - vh + hh));
                         }
-                        const int jj = half * (C::NJ / 2) + ch * 8 + 2 * tt + role;
+                        const int jj = half * JPH + ch * 8 + 2 * tt + role;
                         const int j = j0 + jj;
                         if (row_ok && j > i && j < my_jmax) {
                             const int b = bin_advance(sedges, nb, cur, fabs(a.coord[j] - ci));
@@ -471,9 +477,9 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
                             }
                             if (b >= 0 && b < nb) {
 #pragma unroll
-                                for (int p = 0; p < P; ++p) hap_features<float, P>(f[p]);
-                                hap_stats<float, P>(f, acc);
-                                float r2;
+                                for (int p = 0; p < P; ++p) hap_features<T, P>(f[p]);
+                                hap_stats<T, P>(f, acc);
+                                T r2;
                                 if (hap_r2(f[0], r2)) { r2acc += r2; ++nr2; }
                                 ++np;
                             }
@@ -484,9 +490,9 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
             flush();
             (void)ok;
             // stage -> global, once per row block
-            epi_bar();
+            epi_bar<EPI>();
             const int et = threadIdx.x - 64;
-            for (int idx = et; idx < kSlots * nb * (NS + 1); idx += 32 * kEpiWarps) {
+            for (int idx = et; idx < kSlots * nb * (NS + 1); idx += 32 * EPI) {
                 const int sl = idx / (nb * (NS + 1));
                 const int rem = idx % (nb * (NS + 1));
                 const int bb = rem / (NS + 1), s = rem % (NS + 1);
@@ -498,7 +504,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
                 }
                 sacc[idx] = 0.0;
             }
-            for (int idx = et; idx < kSlots * nb; idx += 32 * kEpiWarps) {
+            for (int idx = et; idx < kSlots * nb; idx += 32 * EPI) {
                 const int blk = blk0 + idx / nb, bb = idx % nb;
                 if (blk < a.n_blocks) {
                     if (scnt[2 * idx]) atomicAdd(&a.pairs[(int64_t)blk * nb + bb], (unsigned long long)scnt[2 * idx]);
@@ -508,7 +514,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
                 scnt[2 * idx] = 0u;
                 scnt[2 * idx + 1] = 0u;
             }
-            epi_bar();
+            epi_bar<EPI>();
         }
     }
     tc_fence_before();
@@ -560,6 +566,15 @@ size_t smem_bytes_t(int nb) {
 
 int tc_rows_per_block(const ParseShape&) { return kRows; }
 
+// Epilogue width of the tensor-core kernel: 4 warps unless LDK_TC_EPI_WARPS=8.
+int tc_epilogue_warps() {
+    static int v = [] {
+        const char* e = getenv("LDK_TC_EPI_WARPS");
+        return (e && atoi(e) == 8) ? 8 : 4;
+    }();
+    return v;
+}
+
 size_t tc_smem_bytes(const ParseShape& sh) {
     switch (sh.P) {
         case 1: return smem_bytes_t<1>(sh.n_bins);
@@ -589,7 +604,7 @@ cudaError_t launch_prep_planes(const ldk_parse_t* d, const Scratch& w, const Par
     return cudaGetLastError();
 }
 
-template <int P>
+template <int P, typename T, int EPI>
 static cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w,
                                      const ParseShape& sh, int n_items, cudaStream_t s) {
     using C = Cfg<P>;
@@ -612,27 +627,39 @@ static cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t
     a.pairs = reinterpret_cast<unsigned long long*>(o->pairs);
     a.r2_counts = reinterpret_cast<unsigned long long*>(o->r2_counts);
     a.status = w.status;
-    const size_t smem = smem_bytes_t<P>(d->n_bins);
-    cudaError_t e = cudaFuncSetAttribute(k_parse_tc<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // at least half of an SM's shared memory, so that one CTA (holding all 512 TMEM
+    // columns) runs per SM
+    size_t smem = smem_bytes_t<P>(d->n_bins);
+    if (smem < kMinSmem) smem = kMinSmem;
+    cudaError_t e = cudaFuncSetAttribute(k_parse_tc<P, T, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (n_items == 0) return cudaSuccess;
     const int grid = n_items < sms ? n_items : sms;
-    k_parse_tc<P><<<grid, kThreadsTC, smem, s>>>(mA, mB, a);
+    k_parse_tc<P, T, EPI><<<grid, 64 + 32 * EPI, smem, s>>>(mA, mB, a);
     return cudaGetLastError();
 }
 
 cudaError_t launch_parse_tc(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w,
                             const ParseShape& sh, int n_items, cudaStream_t s) {
+    const bool f32 = d->method == LDK_METHOD_TC_FP32;
+    const bool wide = tc_epilogue_warps() == 8;
+#define LDK_TC_CASE(PP)                                                                       \
+    case PP:                                                                                  \
+        if (f32) return wide ? launch_parse_tc_p<PP, float, 8>(d, o, w, sh, n_items, s)       \
+                             : launch_parse_tc_p<PP, float, 4>(d, o, w, sh, n_items, s);      \
+        return wide ? launch_parse_tc_p<PP, double, 8>(d, o, w, sh, n_items, s)               \
+                    : launch_parse_tc_p<PP, double, 4>(d, o, w, sh, n_items, s);
     switch (sh.P) {
-        case 1: return launch_parse_tc_p<1>(d, o, w, sh, n_items, s);
-        case 2: return launch_parse_tc_p<2>(d, o, w, sh, n_items, s);
-        case 3: return launch_parse_tc_p<3>(d, o, w, sh, n_items, s);
-        case 4: return launch_parse_tc_p<4>(d, o, w, sh, n_items, s);
+        LDK_TC_CASE(1)
+        LDK_TC_CASE(2)
+        LDK_TC_CASE(3)
+        LDK_TC_CASE(4)
         default: return cudaErrorInvalidValue;
     }
+#undef LDK_TC_CASE
 }
 
 }  // namespace ldk

@@ -17,7 +17,7 @@ import numpy as np
 
 from . import _lib
 
-METHODS = {"plain": _lib.METHOD_PLAIN, "tc": _lib.METHOD_TC}
+METHODS = {"plain": _lib.METHOD_PLAIN, "tc": _lib.METHOD_TC, "tc32": _lib.METHOD_TC_FP32}
 
 
 def n_stats(P: int) -> int:
