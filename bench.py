@@ -1,0 +1,454 @@
+#!/usr/bin/env python
+"""Throughput of the B200 two-locus LD parse: SNP pairs per second.
+
+Workload (default): configuration 4 of the north-star set -- 200 windows of lognormal
+SNP counts (median 2,000, 200..20,000), 3 populations of 50/120/300 haplotypes, 3%
+missing, 16 log-spaced distance bins (10 bp .. 1 Mb), per-window per-bin FP64
+DD/Dz/pi2 (45 statistics), 50-kb bootstrap blocks and 100 block-bootstrap replicates.
+Seeded synthetic data (founder mosaics, see pg_gpu_b200/synth.py).
+
+One step = the whole batched parse of that workload: pair ranges, indicator planes,
+the fused INT8 tcgen05 count + estimator + bin kernel, per-window totals and bootstrap
+replicates.  ``value`` has inputs resident in HBM; ``e2e`` copies the inputs from
+pinned host memory and the results back every step.  ``--impl reference`` times the
+CPU restatement of pg_gpu's path (the oracle) on the host cores instead.
+
+Multi-GPU (torchrun): weak scaling, each rank parses its own independently seeded
+workload of the same shape; no data-path collective.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+import numpy as np  # noqa: E402
+
+METRIC = "LD SNP-pairs/s: INT8-TC+FP32 vs plain FP64 on same B200, rel err ≤1e-6"
+UNIT = "SNP-pairs/s"
+FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+
+def peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return dict(FALLBACK_PEAKS), "fallback"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, phys_index):
+        self.phys = str(phys_index)
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9 or parts[0] != self.phys:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the oracle (pg_gpu's algorithm restated in NumPy) on a bounded sample
+# ---------------------------------------------------------------------------
+
+def _cpu_task(args):
+    data, pos, pop_rows, edges, max_dist, n_pairs = args
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    from oracle import ld_oracle as O
+    t0 = time.perf_counter()
+    r = O.bin_sums(data, pos, pop_rows, edges, max_dist=max_dist, pair_range=(0, n_pairs))
+    return min(n_pairs, r["n_pairs"]), time.perf_counter() - t0
+
+
+def cpu_sample_tasks(w, workers, pairs_per_worker):
+    """One task per worker: the first pairs of a window of <= 3,000 SNPs."""
+    offs = w.window_offsets if w.window_offsets is not None else np.array([0, w.n_var])
+    cand = [k for k in range(len(offs) - 1) if 200 <= offs[k + 1] - offs[k] <= 3000] or [0]
+    tasks = []
+    for t in range(workers):
+        k = cand[t % len(cand)]
+        a, b = int(offs[k]), int(offs[k + 1])
+        tasks.append((np.ascontiguousarray(w.data[:, a:b]), w.positions[a:b].copy(), w.pop_rows, w.edges,
+                      w.max_dist, pairs_per_worker))
+    return tasks
+
+
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_pool(workers):
+    import multiprocessing as mp
+    pool = mp.get_context("spawn").Pool(workers)
+    pool.map(_noop, range(workers))  # start every worker before timing
+    return pool
+
+
+def _noop(_):
+    from oracle import ld_oracle  # noqa: F401
+    return 0
+
+
+def run_cpu_sample(w, seconds, workers=None, pool=None):
+    """Time the oracle on ~``seconds`` of CPU work per worker; pairs/s over all workers."""
+    workers = workers or cpu_cores()
+    probe = cpu_sample_tasks(w, 1, 20_000)[0]
+    n, dt = _cpu_task(probe)
+    rate = n / max(dt, 1e-9)
+    per_worker = max(20_000, int(rate * seconds))
+    tasks = cpu_sample_tasks(w, workers, per_worker)
+    own = pool is None
+    if own:
+        pool = cpu_pool(workers)
+    t0 = time.perf_counter()
+    res = pool.map(_cpu_task, tasks)
+    wall = time.perf_counter() - t0
+    if own:
+        pool.close()
+        pool.join()
+    pairs = sum(r[0] for r in res)
+    return {"value": pairs / wall, "pairs": pairs, "wall_s": wall, "workers": workers,
+            "per_worker_pairs": per_worker}
+
+
+# ---------------------------------------------------------------------------
+# main
+# ---------------------------------------------------------------------------
+
+def make_workload(cfg, scale, rank):
+    from pg_gpu_b200 import synth
+    seed = {1: 1, 2: 2, 3: 3, 4: 4, 5: 5}[cfg] + 1000 * rank
+    return synth.make_config(cfg, scale=scale, seed=seed)
+
+
+def algorithmic_int_ops_per_pair(w):
+    """Count-stage INT ops per pair (MAC = 2): four 0/1 dot products of length n per
+    population with missing data (h.h, h.v, v.h, v.v), i.e. 8n per population."""
+    return sum(8 * len(r) for r in w.pop_rows)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", type=int, default=4)
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--method", choices=["tc", "tc32", "plain"], default="tc")
+    ap.add_argument("--plain-steps", type=int, default=2, help="steps of the plain FP64 kernel for the ratio")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, ws, rank)
+
+    import torch
+    import torch.distributed as dist
+
+    if ws > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    from pg_gpu_b200 import _lib, parse, synth
+
+    lib = _lib.load()
+    w = make_workload(args.config, args.scale, rank)
+    n_pairs = synth.count_pairs(w)
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = run_cpu_sample(w, args.cpu_seconds)
+
+    parser = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, method=args.method, max_dist=w.max_dist,
+                          window_offsets=w.window_offsets, snp_block=w.snp_block, n_blocks=w.n_blocks,
+                          device=dev)
+    reps_w = torch.as_tensor(w.replicate_weights if w.replicate_weights is not None
+                             else np.ones((1, w.n_blocks), np.int32), dtype=torch.int32, device=dev)
+    if w.window_of_block is not None:
+        win_ind = np.zeros((len(w.window_offsets) - 1, w.n_blocks), np.int32)
+        win_ind[w.window_of_block, np.arange(w.n_blocks)] = 1
+    else:
+        win_ind = np.ones((1, w.n_blocks), np.int32)
+    win_w = torch.as_tensor(win_ind, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        r = parser.run()
+        reps = parse.block_combine(r.sums, reps_w)
+        wins = parse.block_combine(r.sums, win_w)
+        return r, reps, wins
+
+    lib.ldk_profile(1)
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    phys = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")
+    phys_index = phys[dev.index] if phys and phys[0] not in ("",) and dev.index < len(phys) else dev.index
+    kernel_ms = []
+    with ClockSampler(phys_index) as clk:
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            r, reps, wins = step()
+            kernel_ms.append(lib.ldk_profile_last_kernel_ms())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+    elapsed_ms = e0.elapsed_time(e1)
+    clocks = clk.summary()
+    t_max = elapsed_ms
+    if ws > 1:
+        t = torch.tensor([elapsed_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    total_pairs = n_pairs * args.steps * ws
+    value = total_pairs / (t_max / 1e3)
+    ms_per_step = t_max / args.steps
+    k_ms = statistics.mean(kernel_ms) if kernel_ms else None
+
+    # ---- end to end through the public API: pinned host inputs in, results out
+    X_h = torch.from_numpy(np.ascontiguousarray(w.data)).pin_memory()
+    pos_h = torch.from_numpy(np.ascontiguousarray(w.positions)).pin_memory()
+    blk_h = torch.from_numpy(np.ascontiguousarray(w.snp_block if w.snp_block is not None
+                                                  else np.zeros(w.n_var, np.int32))).pin_memory()
+    rw_h = reps_w.cpu().pin_memory()
+    out_sums_h = torch.empty(parser.out.sums.shape, dtype=torch.float64).pin_memory()
+    out_reps_h = torch.empty((reps_w.shape[0],) + tuple(parser.out.sums.shape[1:]), dtype=torch.float64).pin_memory()
+    out_wins_h = torch.empty((win_w.shape[0],) + tuple(parser.out.sums.shape[1:]), dtype=torch.float64).pin_memory()
+    out_pairs_h = torch.empty(parser.out.pairs.shape, dtype=torch.int64).pin_memory()
+
+    def e2e_step():
+        parser.X.copy_(X_h, non_blocking=True)
+        parser.pos.copy_(pos_h, non_blocking=True)
+        if parser.block is not None:
+            parser.block.copy_(blk_h, non_blocking=True)
+        reps_w.copy_(rw_h, non_blocking=True)
+        r, reps, wins = step()
+        out_sums_h.copy_(r.sums, non_blocking=True)
+        out_pairs_h.copy_(r.pairs, non_blocking=True)
+        out_reps_h.copy_(reps, non_blocking=True)
+        out_wins_h.copy_(wins, non_blocking=True)
+
+    h2d = X_h.numel() + pos_h.numel() * 8 + (blk_h.numel() * 4 if parser.block is not None else 0) + rw_h.numel() * 4
+    d2h = out_sums_h.numel() * 8 + out_pairs_h.numel() * 8 + out_reps_h.numel() * 8 + out_wins_h.numel() * 8
+    e2e_step()
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    f1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+    if ws > 1:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = total_pairs / (e2e_ms / 1e3)
+
+    # ---- the plain FP64 kernel on the same workload, and parity of the fast path against it
+    plain = None
+    parity = None
+    if args.method != "plain" and args.plain_steps > 0:
+        fast = {k: v.copy() for k, v in parser.out.numpy().items()}
+        pp = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, method="plain", max_dist=w.max_dist,
+                          window_offsets=w.window_offsets, snp_block=w.snp_block, n_blocks=w.n_blocks,
+                          device=dev)
+        pp.run()
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        pk = []
+        for _ in range(args.plain_steps):
+            pp.run()
+            pk.append(lib.ldk_profile_last_kernel_ms())
+        g1.record(stream)
+        torch.cuda.synchronize()
+        pms = g0.elapsed_time(g1) / args.plain_steps
+        if ws > 1:
+            t = torch.tensor([pms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            pms = float(t.item())
+        ref = pp.out.numpy()
+        tot_f, tot_p = fast["sums"].sum(axis=0), ref["sums"].sum(axis=0)
+        parity = {
+            "pairs_bit_exact": bool(np.array_equal(fast["pairs"], ref["pairs"])
+                                    and np.array_equal(fast["r2_counts"], ref["r2_counts"])),
+            "max_rel_err_per_bin": float(np.max(np.abs(tot_f - tot_p) / np.maximum(np.abs(tot_p), 1e-300))),
+            "max_rel_err_per_block_bin": float(np.max(np.abs(fast["sums"] - ref["sums"])
+                                                      / np.maximum(np.abs(ref["sums"]), 1e-300))),
+            "reference": "plain FP64 kernel, same workload",
+        }
+        plain = {"value": n_pairs * ws / (pms / 1e3), "ms_per_step": pms,
+                 "kernel_ms": statistics.mean(pk) if pk else None}
+        del pp
+
+    # ---- roofline of the dominant kernel
+    pk_d, pk_kind = peaks()
+    int8_peak = 2.0 * pk_d["bf16_tflops"]
+    ops = algorithmic_int_ops_per_pair(w) * n_pairs
+    achieved = ops / (k_ms / 1e3) / 1e12 if k_ms else None
+    traffic = None
+    tfile = os.path.join(REPO, "profiles", "k_parse_tc_c4_traffic.json")
+    if os.path.exists(tfile) and args.config == 4 and args.method == "tc":
+        with open(tfile) as f:
+            tj = json.load(f)
+        traffic = tj.get("dram_bytes_per_pair", 0.0) * n_pairs
+    roofline = {"bound": "tensor", "kernel": "k_parse_tc", "achieved": achieved, "peak": int8_peak,
+                "unit": "TOP/s (INT8, MAC=2)", "frac": (achieved / int8_peak) if achieved else None,
+                "peak_source": f"2 x {pk_kind} bf16 dense burst {pk_d['bf16_tflops']} TFLOP/s (derived)",
+                "traffic": traffic, "kernel_ms": k_ms,
+                "note": "count stage algorithmic ops = 8 x sum(n_pop) per pair; the fused kernel is bound by "
+                        "its FP64 estimator epilogue, not by the tensor pipe"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8 counts / s32 accumulate / f64 estimators",
+            "data": "synthetic (seeded founder mosaics; no public dataset offline)",
+            "config": {"workload": w.name, "config_index": args.config, "scale": args.scale,
+                       "snps": int(w.n_var), "pairs_per_step_per_gpu": int(n_pairs),
+                       "populations": [len(r) for r in w.pop_rows], "bins": int(len(w.edges) - 1),
+                       "statistics": int(parse.n_stats(len(w.pop_rows))), "windows":
+                       int(len(w.window_offsets) - 1) if w.window_offsets is not None else 1,
+                       "bootstrap_blocks": int(w.n_blocks),
+                       "bootstrap_replicates": int(reps_w.shape[0]),
+                       "method": args.method, "parallelism": f"weak x{ws}, no data-path collective",
+                       "l2": "inputs larger than L2 (haplotypes %d MB, indicator planes %d MB)" % (
+                           w.data.nbytes >> 20, (w.n_var * 2 * parser_ktot(w)) >> 20)},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "roofline": roofline,
+            "gpu_launches": int(args.steps * (4 if args.method != "plain" else 3)),
+            "clocks": clocks,
+        }
+        if plain:
+            line["plain_fp64"] = plain
+            line["speedup_vs_plain_fp64"] = value / plain["value"]
+        if parity:
+            line["parity"] = parity
+        if cpu:
+            line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["workers"], "kind": "port",
+                                    "sample": f"oracle (NumPy restatement of pg_gpu's path) on the first "
+                                              f"{cpu['per_worker_pairs']} pairs of one window per worker, "
+                                              f"{cpu['workers']} spawn workers, {cpu['wall_s']:.1f} s wall"}
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.destroy_process_group()
+
+
+def parser_ktot(w):
+    k = sum((len(r) + 31) // 32 * 32 for r in w.pop_rows)
+    return (k + 127) // 128 * 128
+
+
+def run_reference(args, ws, rank):
+    """pg_gpu's path restated on the CPU (the oracle), all host cores, bounded samples."""
+    if ws > 1 and rank != 0:
+        return
+    w = make_workload(args.config, args.scale, 0)
+    cores = cpu_cores()
+    per_step = max(5.0, min(args.cpu_seconds, 20.0))
+    pool = cpu_pool(cores)
+    for _ in range(max(0, min(args.warmup, 1))):
+        run_cpu_sample(w, 2.0, cores, pool)
+    vals, pairs, wall = [], 0, 0.0
+    for _ in range(args.steps):
+        r = run_cpu_sample(w, per_step, cores, pool)
+        vals.append(r["value"])
+        pairs += r["pairs"]
+        wall += r["wall_s"]
+    pool.close()
+    pool.join()
+    value = pairs / wall
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded founder mosaics)",
+            "config": {"workload": w.name, "config_index": args.config, "scale": args.scale},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"oracle on the first pairs of one window per worker, {cores} workers, "
+                                       f"~{per_step:.0f} s per step"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -121,6 +121,13 @@ LDK_API size_t ldk_parse_workspace_size(const ldk_parse_t* d);
 LDK_API int ldk_parse(const ldk_parse_t* d, const ldk_parse_out_t* out, void* workspace,
               size_t workspace_bytes, void* stream);
 
+/* Per-thread kernel timing: while enabled, ldk_parse brackets its main counting /
+ * estimator kernel with CUDA events on the caller's stream; ldk_profile_last_kernel_ms
+ * returns that kernel's duration in the calling thread's last ldk_parse (-1 if none).
+ * No counterpart in pg_gpu (measurement support). */
+LDK_API int ldk_profile(int enable);
+LDK_API double ldk_profile_last_kernel_ms(void);
+
 /* out[r, k] = sum_b weights[r, b] * block_sums[b, k] (float64); weights int32 (R, n_blocks).
  * Block-bootstrap replicates over pre-binned per-block sums, the semantics of
  * resampling.block_bootstrap (resampling.py:201-256); also per-window totals. */

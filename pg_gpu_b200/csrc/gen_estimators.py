@@ -677,7 +677,6 @@ def emit_hap(P):
     for n, e in HAP_FEATURES:
         if n in feats:
             L.append(f"    x.{n} = {_cexpr(e)};")
-    L.append("    hap_reciprocals(x);")
     L.append("}")
     L.append("template <typename T>")
     L.append(f"LDK_DEV void hap_stats_P{P}(const HapFeat<T>* f, T* acc) {{")

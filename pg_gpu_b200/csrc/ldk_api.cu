@@ -12,6 +12,22 @@ namespace ldk {
 namespace {
 thread_local char g_err[512] = "";
 
+// Optional timing of the main parse kernel (CUDA events on the caller's stream).
+thread_local int g_prof = 0;
+thread_local float g_kernel_ms = -1.0f;
+thread_local cudaEvent_t g_ev[2] = {nullptr, nullptr};
+thread_local int g_ev_dev = -1;
+
+bool prof_events() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (g_ev[0] && g_ev_dev == dev) return true;
+    if (g_ev[0]) { cudaEventDestroy(g_ev[0]); cudaEventDestroy(g_ev[1]); g_ev[0] = g_ev[1] = nullptr; }
+    if (cudaEventCreate(&g_ev[0]) != cudaSuccess || cudaEventCreate(&g_ev[1]) != cudaSuccess) return false;
+    g_ev_dev = dev;
+    return true;
+}
+
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 int stats_of(int P) { return P == 1 ? 3 : P == 2 ? 15 : P == 3 ? 45 : P == 4 ? 105 : 0; }
@@ -51,11 +67,13 @@ bool shape_of(const ldk_parse_t* d, ParseShape& sh) {
     sh.n_bins = d->n_bins;
     sh.planes = 2;
     int k = 0;
+    sh.max_n = 0;
     for (int p = 0; p < LDK_MAX_POPS + 1; ++p) sh.kofs[p] = 0;
     for (int p = 0; p < d->n_pops; ++p) {
         sh.kofs[p] = k;
         const int np = d->pop_offsets[p + 1] - d->pop_offsets[p];
         k += (np + 31) / 32 * 32;
+        if (np > sh.max_n) sh.max_n = np;
     }
     for (int p = d->n_pops; p <= LDK_MAX_POPS; ++p) sh.kofs[p] = k;
     sh.ktot = (k + 127) / 128 * 128;
@@ -266,8 +284,12 @@ int ldk_parse(const ldk_parse_t* d, const ldk_parse_out_t* out, void* workspace,
     dd.n_windows = window_count(d);
     if ((rc = check_cuda(launch_jmax(&dd, w, s), "pair ranges"))) return rc;
 
+    const bool prof = g_prof && prof_events();
+    g_kernel_ms = -1.0f;
     if (d->method == LDK_METHOD_PLAIN_FP64) {
+        if (prof) cudaEventRecord(g_ev[0], s);
         if ((rc = check_cuda(launch_parse_plain(&dd, out, w, sh, s), "plain parse"))) return rc;
+        if (prof) cudaEventRecord(g_ev[1], s);
     } else {
         // row blocks of 64 SNPs, largest windows first (round-robin over persistent CTAs)
         std::vector<int> order(window_count(d));
@@ -287,19 +309,29 @@ int ldk_parse(const ldk_parse_t* d, const ldk_parse_out_t* out, void* workspace,
                                              cudaMemcpyHostToDevice, s), "upload row blocks")))
             return rc;
         if ((rc = check_cuda(launch_prep_planes(&dd, w, sh, s), "indicator planes"))) return rc;
+        if (prof) cudaEventRecord(g_ev[0], s);
         if ((rc = check_cuda(launch_parse_tc(&dd, out, w, sh, (int)(items.size() / 2), s), "tensor-core parse")))
             return rc;
+        if (prof) cudaEventRecord(g_ev[1], s);
     }
     unsigned status = 0;
     if ((rc = check_cuda(cudaMemcpyAsync(&status, w.status, sizeof(unsigned), cudaMemcpyDeviceToHost, s), "status")))
         return rc;
     if ((rc = check_cuda(cudaStreamSynchronize(s), "ldk_parse"))) return rc;
+    if (prof) cudaEventElapsedTime(&g_kernel_ms, g_ev[0], g_ev[1]);
     if (status) {
         set_error("%s (status 0x%x)", status_text(status), status);
         return LDK_ERR_DEVICE;
     }
     return LDK_OK;
 }
+
+int ldk_profile(int enable) {
+    g_prof = enable ? 1 : 0;
+    return LDK_OK;
+}
+
+double ldk_profile_last_kernel_ms(void) { return (double)g_kernel_ms; }
 
 int ldk_block_combine(const double* block_sums, int64_t n_blocks, int64_t k, const int32_t* weights, int64_t n_rep,
                       double* out, void* stream) {

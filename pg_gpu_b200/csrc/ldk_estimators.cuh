@@ -23,7 +23,6 @@ LDK_DEV void hap_features_P1(HapFeat<T>& x) {
     x.DDs = x.E * x.E - x.c1 * x.c4 * (x.c1 + x.c4 - T(1)) - x.c2 * x.c3 * (x.c2 + x.c3 - T(1));
     x.DZs = x.E * x.a * x.b + x.E * x.s + T(2) * (x.c2 * x.c3 + x.c1 * x.c4);
     x.PIs = x.fA * x.fB - x.c1 * x.c4 * (-T(1) + x.c1 + T(3) * x.c2 + T(3) * x.c3 + x.c4) - x.c2 * x.c3 * (-T(1) + T(3) * x.c1 + x.c2 + x.c3 + T(3) * x.c4);
-    hap_reciprocals(x);
 }
 template <typename T>
 LDK_DEV void hap_stats_P1(const HapFeat<T>* f, T* acc) {
@@ -61,7 +60,6 @@ LDK_DEV void hap_features_P2(HapFeat<T>& x) {
     x.DDs = x.E * x.E - x.c1 * x.c4 * (x.c1 + x.c4 - T(1)) - x.c2 * x.c3 * (x.c2 + x.c3 - T(1));
     x.DZs = x.E * x.a * x.b + x.E * x.s + T(2) * (x.c2 * x.c3 + x.c1 * x.c4);
     x.PIs = x.fA * x.fB - x.c1 * x.c4 * (-T(1) + x.c1 + T(3) * x.c2 + T(3) * x.c3 + x.c4) - x.c2 * x.c3 * (-T(1) + T(3) * x.c1 + x.c2 + x.c3 + T(3) * x.c4);
-    hap_reciprocals(x);
 }
 template <typename T>
 LDK_DEV void hap_stats_P2(const HapFeat<T>* f, T* acc) {
@@ -127,7 +125,6 @@ LDK_DEV void hap_features_P3(HapFeat<T>& x) {
     x.DDs = x.E * x.E - x.c1 * x.c4 * (x.c1 + x.c4 - T(1)) - x.c2 * x.c3 * (x.c2 + x.c3 - T(1));
     x.DZs = x.E * x.a * x.b + x.E * x.s + T(2) * (x.c2 * x.c3 + x.c1 * x.c4);
     x.PIs = x.fA * x.fB - x.c1 * x.c4 * (-T(1) + x.c1 + T(3) * x.c2 + T(3) * x.c3 + x.c4) - x.c2 * x.c3 * (-T(1) + T(3) * x.c1 + x.c2 + x.c3 + T(3) * x.c4);
-    hap_reciprocals(x);
 }
 template <typename T>
 LDK_DEV void hap_stats_P3(const HapFeat<T>* f, T* acc) {
@@ -270,7 +267,6 @@ LDK_DEV void hap_features_P4(HapFeat<T>& x) {
     x.DDs = x.E * x.E - x.c1 * x.c4 * (x.c1 + x.c4 - T(1)) - x.c2 * x.c3 * (x.c2 + x.c3 - T(1));
     x.DZs = x.E * x.a * x.b + x.E * x.s + T(2) * (x.c2 * x.c3 + x.c1 * x.c4);
     x.PIs = x.fA * x.fB - x.c1 * x.c4 * (-T(1) + x.c1 + T(3) * x.c2 + T(3) * x.c3 + x.c4) - x.c2 * x.c3 * (-T(1) + T(3) * x.c1 + x.c2 + x.c3 + T(3) * x.c4);
-    hap_reciprocals(x);
 }
 template <typename T>
 LDK_DEV void hap_stats_P4(const HapFeat<T>* f, T* acc) {

@@ -32,6 +32,26 @@ LDK_DEV void hap_reciprocals(HapFeat<T>& x) {
     }
 }
 
+// Reciprocal table entry for sample size n: {1/n, 1/(n(n-1)), 1/(n(n-1)(n-2)),
+// 1/(n(n-1)(n-2)(n-3))}, each 0 where its product is 0 (built once per CTA).
+LDK_DEV double4 recip_entry(int n) {
+    const double d = (double)n;
+    double4 r;
+    r.x = n >= 1 ? 1.0 / d : 0.0;
+    r.y = n >= 2 ? 1.0 / (d * (d - 1.0)) : 0.0;
+    r.z = n >= 3 ? 1.0 / (d * (d - 1.0) * (d - 2.0)) : 0.0;
+    r.w = n >= 4 ? 1.0 / (d * (d - 1.0) * (d - 2.0) * (d - 3.0)) : 0.0;
+    return r;
+}
+
+template <typename T>
+LDK_DEV void hap_reciprocals_from(HapFeat<T>& x, const double4& r) {
+    x.r1 = T(r.x);
+    x.r2 = T(r.y);
+    x.r3 = T(r.z);
+    x.r4 = T(r.w);
+}
+
 template <typename T>
 LDK_DEV void hap_set_counts(HapFeat<T>& x, T c1, T c2, T c3, T c4) {
     x.c1 = c1; x.c2 = c2; x.c3 = c3; x.c4 = c4;

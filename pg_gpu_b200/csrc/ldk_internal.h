@@ -26,6 +26,7 @@ struct ParseShape {
     int kofs[LDK_MAX_POPS + 1];  // TC path: K offset (bytes) of each population segment
     int ktot;                    // TC path: total K bytes (multiple of 128)
     int planes;                  // TC path: indicator planes per SNP (2 haplotype, 4 genotype)
+    int max_n;                   // largest population size
 };
 
 // launchers (ldk_plain.cu)

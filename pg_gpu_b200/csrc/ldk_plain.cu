@@ -97,6 +97,7 @@ __global__ void k_stats_hap(const int32_t* __restrict__ counts, const int32_t* _
             hap_set_counts(f[p], double(c.x), double(c.y), double(c.z), double(c.w));
             if (n_valid) f[p].n = double(n_valid[p * n + t]);
             hap_features<double, P>(f[p]);
+            hap_reciprocals(f[p]);
         }
         double acc[NS];
 #pragma unroll
@@ -146,6 +147,7 @@ __global__ void k_raw_hap(int case_id, RawArgs args, int P_total, const double* 
             hap_set_counts(f[p], c[0], c[1], c[2], c[3]);
             if (n_valid) f[p].n = n_valid[t * P_total + p];
             hap_features<double, 4>(f[p]);
+            hap_reciprocals(f[p]);
         }
         out[t] = hap_raw_by_case<double>(case_id, args.g, f);
     }
@@ -316,6 +318,7 @@ __global__ void __launch_bounds__(kThreads) k_parse_plain(PlainArgs a) {
                             hap_set_counts(f[p], double(c11), double(c10), double(c01), double(c00));
                             f[p].n = double(nv);
                             hap_features<double, P>(f[p]);
+                            hap_reciprocals(f[p]);
                         }
                         hap_stats<double, P>(f, v);
                         r2ok = hap_r2(f[0], r2);

@@ -269,6 +269,7 @@ struct TcArgs {
     int n_items;
     int nkc;               // K chunks of 128 bytes
     int kofs[LDK_MAX_POPS + 1];
+    int max_n;             // largest population (reciprocal table size - 1)
     BinEdges edges;
     double* sums;
     double* r2_sums;
@@ -278,7 +279,7 @@ struct TcArgs {
 };
 
 template <int P, typename T, int EPI>
-__global__ void __maxnreg__(EPI == 8 ? 192 : 255)
+__global__ void __launch_bounds__(128 + 32 * EPI, 1)
     k_parse_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcArgs a) {
     using C = Cfg<P>;
     constexpr int NS = C::NS;
@@ -288,6 +289,7 @@ __global__ void __maxnreg__(EPI == 8 ? 192 : 255)
     unsigned char* stages = base;
     double* sacc = reinterpret_cast<double*>(base + C::STAGES * C::STAGE_BYTES);      // [kSlots][nb][NS+1]
     unsigned* scnt = reinterpret_cast<unsigned*>(sacc + kSlots * nb * (NS + 1));        // [kSlots][nb][2]
+    double4* rtab = reinterpret_cast<double4*>(scnt + ((kSlots * nb * 2 + 7) & ~7));     // [max_n + 1]
 
     __shared__ __align__(8) uint64_t full_bar[C::STAGES], empty_bar[C::STAGES], tfull[2], tempty[2];
     __shared__ uint32_t tmem_base_s;
@@ -310,6 +312,7 @@ __global__ void __maxnreg__(EPI == 8 ? 192 : 255)
     for (int b = threadIdx.x; b <= nb; b += blockDim.x) sedges[b] = a.edges.e[b];
     for (int idx = threadIdx.x; idx < kSlots * nb * (NS + 1); idx += blockDim.x) sacc[idx] = 0.0;
     for (int idx = threadIdx.x; idx < kSlots * nb * 2; idx += blockDim.x) scnt[idx] = 0u;
+    for (int idx = threadIdx.x; idx <= a.max_n; idx += blockDim.x) rtab[idx] = recip_entry(idx);
     if (warp == 1) {
         tmem_alloc(&tmem_base_s, kTmemCols);
         tmem_relinquish();
@@ -318,6 +321,13 @@ __global__ void __maxnreg__(EPI == 8 ? 192 : 255)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_base_s;
+    if constexpr (EPI == 8) {
+        // Rebalance the register file before any role waits on another: the control
+        // warpgroup gives up registers first (4 x 32 x 56 + 8 x 32 x 224 = 384 x 168, the
+        // launch allocation checked on the host), the epilogue warpgroups take them.
+        if (warp < 4) asm volatile("setmaxnreg.dec.sync.aligned.u32 56;");
+        else asm volatile("setmaxnreg.inc.sync.aligned.u32 224;");
+    }
 
     if (warp == 0) {
         // ------------------------------------------------------------- TMA producer
@@ -384,11 +394,12 @@ __global__ void __maxnreg__(EPI == 8 ? 192 : 255)
             if (!ok) spin_ns(2000000);
         }
         __syncwarp();
-    } else {
+    }
+    if (warp >= 4) {
         // ------------------------------------------------------------- epilogue
         constexpr int HALVES = EPI / 4;
         constexpr int JPH = C::NJ / HALVES;  // partners per thread group
-        const int e = warp - 2;
+        const int e = warp - 4;
         const int quarter = warp & 3, half = e >> 2;
         const int L = quarter * 32 + lane;
         const int r = L >> 1, role = L & 1;
@@ -455,6 +466,7 @@ __global__ void __maxnreg__(EPI == 8 ? 192 : 255)
 #pragma unroll 1
                     for (int tt = 0; tt < 4; ++tt) {
                         HapFeat<T> f[P];
+                        int nval[P];
 #pragma unroll
                         for (int p = 0; p < P; ++p) {
                             // lane 2r: (hh, hv) of partners 2tt, 2tt+1; lane 2r+1: (vh, vv)
@@ -466,6 +478,7 @@ __global__ void __maxnreg__(EPI == 8 ? 192 : 255)
                             if (role == 0) { hh = (int)v[p][4 * tt]; hv = (int)v[p][4 * tt + 1]; vh = (int)rx; vv = (int)ry; }
                             else { vh = (int)v[p][4 * tt + 2]; vv = (int)v[p][4 * tt + 3]; hh = (int)rx; hv = (int)ry; }
                             hap_set_counts(f[p], T(hh), T(hv - hh), T(vh - hh), T(vv - hv - vh + hh));
+                            nval[p] = vv;
                         }
                         const int jj = half * JPH + ch * 8 + 2 * tt + role;
                         const int j = j0 + jj;
@@ -477,7 +490,10 @@ __global__ void __maxnreg__(EPI == 8 ? 192 : 255)
                             }
                             if (b >= 0 && b < nb) {
 #pragma unroll
-                                for (int p = 0; p < P; ++p) hap_features<T, P>(f[p]);
+                                for (int p = 0; p < P; ++p) {
+                                    hap_features<T, P>(f[p]);
+                                    hap_reciprocals_from(f[p], rtab[nval[p]]);
+                                }
                                 hap_stats<T, P>(f, acc);
                                 T r2;
                                 if (hap_r2(f[0], r2)) { r2acc += r2; ++nr2; }
@@ -491,7 +507,7 @@ __global__ void __maxnreg__(EPI == 8 ? 192 : 255)
             (void)ok;
             // stage -> global, once per row block
             epi_bar<EPI>();
-            const int et = threadIdx.x - 64;
+            const int et = threadIdx.x - 128;
             for (int idx = et; idx < kSlots * nb * (NS + 1); idx += 32 * EPI) {
                 const int sl = idx / (nb * (NS + 1));
                 const int rem = idx % (nb * (NS + 1));
@@ -556,10 +572,10 @@ bool make_map(CUtensorMap* m, const uint8_t* planes, int64_t n_var, int ktot, in
 }
 
 template <int P>
-size_t smem_bytes_t(int nb) {
+size_t smem_bytes_t(int nb, int max_n) {
     using C = Cfg<P>;
     return 1024 + (size_t)C::STAGES * C::STAGE_BYTES + (size_t)kSlots * nb * (C::NS + 1) * sizeof(double) +
-           (size_t)kSlots * nb * 2 * sizeof(unsigned);
+           (size_t)((kSlots * nb * 2 + 7) & ~7) * sizeof(unsigned) + (size_t)(max_n + 1) * sizeof(double4) + 32;
 }
 
 }  // namespace
@@ -577,10 +593,10 @@ int tc_epilogue_warps() {
 
 size_t tc_smem_bytes(const ParseShape& sh) {
     switch (sh.P) {
-        case 1: return smem_bytes_t<1>(sh.n_bins);
-        case 2: return smem_bytes_t<2>(sh.n_bins);
-        case 3: return smem_bytes_t<3>(sh.n_bins);
-        default: return smem_bytes_t<4>(sh.n_bins);
+        case 1: return smem_bytes_t<1>(sh.n_bins, sh.max_n);
+        case 2: return smem_bytes_t<2>(sh.n_bins, sh.max_n);
+        case 3: return smem_bytes_t<3>(sh.n_bins, sh.max_n);
+        default: return smem_bytes_t<4>(sh.n_bins, sh.max_n);
     }
 }
 
@@ -620,6 +636,7 @@ static cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t
     a.n_items = n_items;
     a.nkc = sh.ktot / kKChunk;
     for (int p = 0; p <= LDK_MAX_POPS; ++p) a.kofs[p] = sh.kofs[p];
+    a.max_n = sh.max_n;
     a.edges.n_bins = d->n_bins;
     for (int b = 0; b <= LDK_MAX_BINS; ++b) a.edges.e[b] = b <= d->n_bins ? d->edges[b] : 0.0;
     a.sums = o->sums;
@@ -629,16 +646,22 @@ static cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t
     a.status = w.status;
     // at least half of an SM's shared memory, so that one CTA (holding all 512 TMEM
     // columns) runs per SM
-    size_t smem = smem_bytes_t<P>(d->n_bins);
+    size_t smem = smem_bytes_t<P>(d->n_bins, sh.max_n);
     if (smem < kMinSmem) smem = kMinSmem;
     cudaError_t e = cudaFuncSetAttribute(k_parse_tc<P, T, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    if (EPI == 8) {
+        // the setmaxnreg split inside the kernel assumes exactly 168 registers per thread
+        cudaFuncAttributes fa;
+        if (cudaFuncGetAttributes(&fa, k_parse_tc<P, T, EPI>) != cudaSuccess || fa.numRegs != 168)
+            return cudaErrorInvalidConfiguration;
+    }
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (n_items == 0) return cudaSuccess;
     const int grid = n_items < sms ? n_items : sms;
-    k_parse_tc<P, T, EPI><<<grid, 64 + 32 * EPI, smem, s>>>(mA, mB, a);
+    k_parse_tc<P, T, EPI><<<grid, 128 + 32 * EPI, smem, s>>>(mA, mB, a);
     return cudaGetLastError();
 }
 
