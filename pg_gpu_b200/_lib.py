@@ -20,6 +20,7 @@ LDK_ERR_WORKSPACE = -4
 LDK_ERR_DEVICE = -5
 LDK_ERR_UNSUPPORTED = -6
 MAX_POPS = 4
+NOALLOC_SCRATCH_BYTES = 64 << 20
 MAX_BINS = 64
 METHOD_PLAIN = 0
 METHOD_TC = 1
@@ -69,6 +70,7 @@ EXPORTS = {
     "ldk_parse_workspace_size": (ctypes.c_size_t, [ctypes.POINTER(ParseDesc)]),
     "ldk_parse": (ctypes.c_int, [ctypes.POINTER(ParseDesc), ctypes.POINTER(ParseOut), c_vp, ctypes.c_size_t,
                                  c_vp]),
+    "ldk_parse_noalloc": (ctypes.c_int, [ctypes.POINTER(ParseDesc), ctypes.POINTER(ParseOut), c_vp]),
     "ldk_profile": (ctypes.c_int, [ctypes.c_int]),
     "ldk_profile_last_kernel_ms": (ctypes.c_double, []),
     "ldk_block_combine": (ctypes.c_int, [c_vp, ctypes.c_int64, ctypes.c_int64, c_vp, ctypes.c_int64, c_vp,

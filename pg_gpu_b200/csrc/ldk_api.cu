@@ -167,6 +167,104 @@ void set_error(const char* fmt, ...) {
 
 using namespace ldk;
 
+int ldk::parse_impl(const ldk_parse_t* d, const ldk_parse_out_t* out, void* workspace, size_t workspace_bytes,
+                    void* stream, bool device_items) {
+    if (int rc = validate(d)) return rc;
+    if (!out || !out->sums || !out->r2_sums || !out->pairs || !out->r2_counts) {
+        set_error("null output pointer");
+        return LDK_ERR_ARG;
+    }
+    ParseShape sh;
+    shape_of(d, sh);
+    const Layout L = layout_of(d, sh);
+    if (!workspace || workspace_bytes < L.total) {
+        set_error("workspace of %zu bytes is smaller than the %zu required", workspace_bytes, L.total);
+        return LDK_ERR_WORKSPACE;
+    }
+    if (reinterpret_cast<uintptr_t>(workspace) % 256) { set_error("workspace must be 256-byte aligned"); return LDK_ERR_ARG; }
+    if (int rc = check_arch()) return rc;
+    if (d->method != LDK_METHOD_PLAIN_FP64 && tc_smem_bytes(sh) > 227 * 1024) {
+        set_error("bins x statistics exceed the tensor-core kernel's shared-memory staging");
+        return LDK_ERR_UNSUPPORTED;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned char* ws = static_cast<unsigned char*>(workspace);
+    Scratch w;
+    w.status = reinterpret_cast<unsigned*>(ws + L.status_off);
+    w.row_counter = reinterpret_cast<int*>(ws + L.status_off + 64);
+    w.jmax = reinterpret_cast<int32_t*>(ws + L.jmax_off);
+    w.win_off = reinterpret_cast<int64_t*>(ws + L.win_off);
+    w.items = reinterpret_cast<int32_t*>(ws + L.items_off);
+    w.hv = ws + L.hv_off;
+
+    const int nb = d->n_bins, NS = stats_of(d->n_pops);
+    int rc;
+    if ((rc = check_cuda(cudaMemsetAsync(out->sums, 0, sizeof(double) * d->n_blocks * nb * NS, s), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(out->r2_sums, 0, sizeof(double) * d->n_blocks * nb, s), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(out->pairs, 0, sizeof(uint64_t) * d->n_blocks * nb, s), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(out->r2_counts, 0, sizeof(uint64_t) * d->n_blocks * nb, s), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(ws + L.status_off, 0, 256, s), "memset")))
+        return rc;
+    if (d->n_var < 2) return LDK_OK;
+
+    std::vector<int64_t> woff(window_count(d) + 1);
+    for (int k = 0; k <= window_count(d); ++k) woff[k] = window_bound(d, k);
+    if ((rc = check_cuda(cudaMemcpyAsync(w.win_off, woff.data(), woff.size() * sizeof(int64_t),
+                                         cudaMemcpyHostToDevice, s), "upload windows")))
+        return rc;
+    ldk_parse_t dd = *d;
+    dd.n_windows = window_count(d);
+    if ((rc = check_cuda(launch_jmax(&dd, w, s), "pair ranges"))) return rc;
+
+    const bool prof = !device_items && g_prof && prof_events();
+    g_kernel_ms = -1.0f;
+    if (d->method == LDK_METHOD_PLAIN_FP64) {
+        if (prof) cudaEventRecord(g_ev[0], s);
+        if ((rc = check_cuda(launch_parse_plain(&dd, out, w, sh, s), "plain parse"))) return rc;
+        if (prof) cudaEventRecord(g_ev[1], s);
+    } else {
+        if (device_items) {
+            // row blocks of 64 SNPs in window order, listed on the device
+            if ((rc = check_cuda(launch_build_items(w, dd.n_windows, s), "row blocks"))) return rc;
+        } else {
+            // row blocks of 64 SNPs, largest windows first (round-robin over persistent CTAs)
+            std::vector<int> order(window_count(d));
+            for (int k = 0; k < (int)order.size(); ++k) order[k] = k;
+            std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+                return (woff[x + 1] - woff[x]) > (woff[y + 1] - woff[y]);
+            });
+            std::vector<int32_t> items;
+            items.reserve((size_t)L.n_items * 2);
+            for (int wi : order)
+                for (int64_t r0 = woff[wi]; r0 < woff[wi + 1]; r0 += 64) {
+                    items.push_back((int32_t)r0);
+                    items.push_back((int32_t)std::min<int64_t>(r0 + 64, woff[wi + 1]));
+                }
+            if (!items.empty() &&
+                (rc = check_cuda(cudaMemcpyAsync(w.items, items.data(), items.size() * sizeof(int32_t),
+                                                 cudaMemcpyHostToDevice, s), "upload row blocks")))
+                return rc;
+        }
+        if ((rc = check_cuda(launch_prep_planes(&dd, w, sh, s), "indicator planes"))) return rc;
+        if (prof) cudaEventRecord(g_ev[0], s);
+        if ((rc = check_cuda(launch_parse_tc(&dd, out, w, sh, L.n_items, s), "tensor-core parse")))
+            return rc;
+        if (prof) cudaEventRecord(g_ev[1], s);
+    }
+    unsigned status = 0;
+    if ((rc = check_cuda(cudaMemcpyAsync(&status, w.status, sizeof(unsigned), cudaMemcpyDeviceToHost, s), "status")))
+        return rc;
+    if ((rc = check_cuda(cudaStreamSynchronize(s), "ldk_parse"))) return rc;
+    if (prof) cudaEventElapsedTime(&g_kernel_ms, g_ev[0], g_ev[1]);
+    if (status) {
+        set_error("%s (status 0x%x)", status_text(status), status);
+        return LDK_ERR_DEVICE;
+    }
+    return LDK_OK;
+}
+
+
+
 extern "C" {
 
 int ldk_version(void) { return 10000; }
@@ -237,93 +335,7 @@ size_t ldk_parse_workspace_size(const ldk_parse_t* d) {
 
 int ldk_parse(const ldk_parse_t* d, const ldk_parse_out_t* out, void* workspace, size_t workspace_bytes,
               void* stream) {
-    if (int rc = validate(d)) return rc;
-    if (!out || !out->sums || !out->r2_sums || !out->pairs || !out->r2_counts) {
-        set_error("null output pointer");
-        return LDK_ERR_ARG;
-    }
-    ParseShape sh;
-    shape_of(d, sh);
-    const Layout L = layout_of(d, sh);
-    if (!workspace || workspace_bytes < L.total) {
-        set_error("workspace of %zu bytes is smaller than the %zu required", workspace_bytes, L.total);
-        return LDK_ERR_WORKSPACE;
-    }
-    if (reinterpret_cast<uintptr_t>(workspace) % 256) { set_error("workspace must be 256-byte aligned"); return LDK_ERR_ARG; }
-    if (int rc = check_arch()) return rc;
-    if (d->method != LDK_METHOD_PLAIN_FP64 && tc_smem_bytes(sh) > 227 * 1024) {
-        set_error("bins x statistics exceed the tensor-core kernel's shared-memory staging");
-        return LDK_ERR_UNSUPPORTED;
-    }
-    cudaStream_t s = (cudaStream_t)stream;
-    unsigned char* ws = static_cast<unsigned char*>(workspace);
-    Scratch w;
-    w.status = reinterpret_cast<unsigned*>(ws + L.status_off);
-    w.row_counter = reinterpret_cast<int*>(ws + L.status_off + 64);
-    w.jmax = reinterpret_cast<int32_t*>(ws + L.jmax_off);
-    w.win_off = reinterpret_cast<int64_t*>(ws + L.win_off);
-    w.items = reinterpret_cast<int32_t*>(ws + L.items_off);
-    w.hv = ws + L.hv_off;
-
-    const int nb = d->n_bins, NS = stats_of(d->n_pops);
-    int rc;
-    if ((rc = check_cuda(cudaMemsetAsync(out->sums, 0, sizeof(double) * d->n_blocks * nb * NS, s), "memset")) ||
-        (rc = check_cuda(cudaMemsetAsync(out->r2_sums, 0, sizeof(double) * d->n_blocks * nb, s), "memset")) ||
-        (rc = check_cuda(cudaMemsetAsync(out->pairs, 0, sizeof(uint64_t) * d->n_blocks * nb, s), "memset")) ||
-        (rc = check_cuda(cudaMemsetAsync(out->r2_counts, 0, sizeof(uint64_t) * d->n_blocks * nb, s), "memset")) ||
-        (rc = check_cuda(cudaMemsetAsync(ws + L.status_off, 0, 256, s), "memset")))
-        return rc;
-    if (d->n_var < 2) return LDK_OK;
-
-    std::vector<int64_t> woff(window_count(d) + 1);
-    for (int k = 0; k <= window_count(d); ++k) woff[k] = window_bound(d, k);
-    if ((rc = check_cuda(cudaMemcpyAsync(w.win_off, woff.data(), woff.size() * sizeof(int64_t),
-                                         cudaMemcpyHostToDevice, s), "upload windows")))
-        return rc;
-    ldk_parse_t dd = *d;
-    dd.n_windows = window_count(d);
-    if ((rc = check_cuda(launch_jmax(&dd, w, s), "pair ranges"))) return rc;
-
-    const bool prof = g_prof && prof_events();
-    g_kernel_ms = -1.0f;
-    if (d->method == LDK_METHOD_PLAIN_FP64) {
-        if (prof) cudaEventRecord(g_ev[0], s);
-        if ((rc = check_cuda(launch_parse_plain(&dd, out, w, sh, s), "plain parse"))) return rc;
-        if (prof) cudaEventRecord(g_ev[1], s);
-    } else {
-        // row blocks of 64 SNPs, largest windows first (round-robin over persistent CTAs)
-        std::vector<int> order(window_count(d));
-        for (int k = 0; k < (int)order.size(); ++k) order[k] = k;
-        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-            return (woff[x + 1] - woff[x]) > (woff[y + 1] - woff[y]);
-        });
-        std::vector<int32_t> items;
-        items.reserve((size_t)L.n_items * 2);
-        for (int wi : order)
-            for (int64_t r0 = woff[wi]; r0 < woff[wi + 1]; r0 += 64) {
-                items.push_back((int32_t)r0);
-                items.push_back((int32_t)std::min<int64_t>(r0 + 64, woff[wi + 1]));
-            }
-        if (!items.empty() &&
-            (rc = check_cuda(cudaMemcpyAsync(w.items, items.data(), items.size() * sizeof(int32_t),
-                                             cudaMemcpyHostToDevice, s), "upload row blocks")))
-            return rc;
-        if ((rc = check_cuda(launch_prep_planes(&dd, w, sh, s), "indicator planes"))) return rc;
-        if (prof) cudaEventRecord(g_ev[0], s);
-        if ((rc = check_cuda(launch_parse_tc(&dd, out, w, sh, (int)(items.size() / 2), s), "tensor-core parse")))
-            return rc;
-        if (prof) cudaEventRecord(g_ev[1], s);
-    }
-    unsigned status = 0;
-    if ((rc = check_cuda(cudaMemcpyAsync(&status, w.status, sizeof(unsigned), cudaMemcpyDeviceToHost, s), "status")))
-        return rc;
-    if ((rc = check_cuda(cudaStreamSynchronize(s), "ldk_parse"))) return rc;
-    if (prof) cudaEventElapsedTime(&g_kernel_ms, g_ev[0], g_ev[1]);
-    if (status) {
-        set_error("%s (status 0x%x)", status_text(status), status);
-        return LDK_ERR_DEVICE;
-    }
-    return LDK_OK;
+    return parse_impl(d, out, workspace, workspace_bytes, stream, false);
 }
 
 int ldk_profile(int enable) {

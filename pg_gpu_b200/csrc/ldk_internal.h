@@ -54,6 +54,13 @@ int tc_rows_per_block(const ParseShape& sh);
 int tc_epilogue_warps();
 size_t tc_smem_bytes(const ParseShape& sh);
 
+cudaError_t launch_build_items(const Scratch& w, int n_windows, cudaStream_t s);
+
+// ldk_parse with a caller-provided workspace; device_items lists the tensor-core row
+// blocks with a device kernel (window order) instead of a host-built upload.
+int parse_impl(const ldk_parse_t* d, const ldk_parse_out_t* out, void* workspace, size_t workspace_bytes,
+               void* stream, bool device_items);
+
 void set_error(const char* fmt, ...);
 
 }  // namespace ldk

@@ -409,6 +409,19 @@ cudaError_t launch_parse_plain_t(const PlainArgs& a, int nb, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// Row blocks of 64 SNPs per window, in window order (one thread: a setup step).
+__global__ void k_build_items(const int64_t* __restrict__ win_off, int n_win, int32_t* __restrict__ items) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    int k = 0;
+    for (int wi = 0; wi < n_win; ++wi)
+        for (int64_t r0 = win_off[wi]; r0 < win_off[wi + 1]; r0 += 64) {
+            items[2 * k] = (int32_t)r0;
+            const int64_t r1 = r0 + 64 < win_off[wi + 1] ? r0 + 64 : win_off[wi + 1];
+            items[2 * k + 1] = (int32_t)r1;
+            ++k;
+        }
+}
+
 __global__ void k_block_combine(const double* __restrict__ block_sums, int64_t n_blocks, int64_t k,
                                 const int32_t* __restrict__ weights, int64_t n_rep, double* __restrict__ out) {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_rep * k;
@@ -510,6 +523,11 @@ cudaError_t launch_parse_plain(const ldk_parse_t* d, const ldk_parse_out_t* o, c
         default: return cudaErrorInvalidValue;
     }
 #undef LDK_PLAIN_CASE
+}
+
+cudaError_t launch_build_items(const Scratch& w, int n_windows, cudaStream_t s) {
+    k_build_items<<<1, 1, 0, s>>>(w.win_off, n_windows, w.items);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_block_combine(const double* block_sums, int64_t n_blocks, int64_t k, const int32_t* weights,
