@@ -371,7 +371,8 @@ def main():
     if os.path.exists(tfile) and args.config == 4 and args.method == "tc":
         with open(tfile) as f:
             tj = json.load(f)
-        traffic = tj.get("dram_bytes_per_pair", 0.0) * n_pairs
+        # captured on this full-size workload: bytes per launch as measured
+        traffic = tj["dram_bytes_per_launch"] if tj.get("pairs") == n_pairs else None
     roofline = {"bound": "tensor", "kernel": "k_parse_tc", "achieved": achieved, "peak": int8_peak,
                 "unit": "TOP/s (INT8, MAC=2)", "frac": (achieved / int8_peak) if achieved else None,
                 "peak_source": f"2 x {pk_kind} bf16 dense burst {pk_d['bf16_tflops']} TFLOP/s (derived)",

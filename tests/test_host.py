@@ -1,0 +1,74 @@
+"""Host-side logic of the drop-in modules (no GPU): VCF and population-file readers,
+biallelic filters, statistic names/specs, chunk sizing, genetic-map helpers."""
+import json
+import os
+
+import numpy as np
+
+from oracle import ld_oracle as O
+from pg_gpu_b200 import genotype_matrix, haplotype_matrix, ld_pipeline, moments_ld
+
+VCF = """##fileformat=VCFv4.2
+#CHROM\tPOS\tID\tREF\tALT\tQUAL\tFILTER\tINFO\tFORMAT\ts0\ts1\ts2
+1\t10\t.\tA\tT\t.\tPASS\t.\tGT\t0|1\t1|1\t0|0
+1\t25\t.\tA\tC\t.\tPASS\t.\tGT\t0|0\t0|0\t0|0
+1\t40\t.\tG\tA\t.\tPASS\t.\tGT\t.|1\t0|1\t1|0
+1\t55\t.\tG\tA,T\t.\tPASS\t.\tGT\t0|2\t0|1\t1|0
+1\t90\t.\tC\tG\t.\tPASS\t.\tGT\t1|0:30\t0|1:20\t1|1:10
+"""
+
+
+def test_vcf_reader_layout_and_filter(tmp_path):
+    p = tmp_path / "x.vcf"
+    p.write_text(VCF)
+    hm = haplotype_matrix.HaplotypeMatrix.from_vcf(str(p))
+    assert hm.num_haplotypes == 6 and hm.num_variants == 5
+    # first alleles of all samples, then second alleles (haplotype_matrix.py:326-329)
+    np.testing.assert_array_equal(hm.haplotypes[:, 0], [0, 1, 0, 1, 1, 0])
+    assert hm.haplotypes[0, 2] == -1
+    f = hm.apply_biallelic_filter()
+    keep = O.biallelic_keep(hm.haplotypes)
+    np.testing.assert_array_equal(np.asarray(f.positions), hm.positions[keep])
+    assert list(np.asarray(f.positions)) == [10, 40, 90]
+    pf = tmp_path / "pops.txt"
+    pf.write_text("sample\tpop\ns0\tA\ns1\tB\ns2\tA\n")
+    hm.load_pop_file(str(pf))
+    assert hm.sample_sets == {"A": [0, 3, 2, 5], "B": [1, 4]}
+    gm = genotype_matrix.GenotypeMatrix.from_haplotype_matrix(f)
+    np.testing.assert_array_equal(gm.genotypes[:, 0], [1, 1, 1])  # rows (0,1), (2,3), (4,5)
+
+
+def test_genotype_filter_matches_oracle():
+    rng = np.random.default_rng(1)
+    g = rng.integers(-1, 3, size=(30, 200)).astype(np.int8)
+    g[:, :20] = 0
+    gm = genotype_matrix.GenotypeMatrix(g, np.arange(200))
+    np.testing.assert_array_equal(gm.biallelic_keep(), O.geno_biallelic_keep(g))
+    np.testing.assert_array_equal(gm.biallelic_keep(rows=range(10)), O.geno_biallelic_keep(g, range(10)))
+
+
+def test_names_specs_match_reference(golden_dir):
+    with open(os.path.join(golden_dir, "ref_names.json")) as f:
+        ref = json.load(f)
+    for P in (1, 2, 3, 4):
+        assert ld_pipeline.ld_names(P) == ref[str(P)]["ld"]
+        assert ld_pipeline.het_names(P) == ref[str(P)]["het"]
+        mine = [[n, [[w, k, list(q)] for (w, k, q) in calls]] for n, calls in ld_pipeline.generate_stat_specs(P)]
+        assert mine == ref[str(P)]["specs"]
+
+
+def test_chunk_size_model():
+    assert ld_pipeline.estimate_ld_chunk_size(100, available_memory_bytes=10 ** 9) == 10 ** 9 // ((4 * 100 * 2 + 300) * 3)
+    assert ld_pipeline.estimate_ld_chunk_size(100, available_memory_bytes=10) == 100_000
+    assert ld_pipeline.estimate_ld_chunk_size(1, available_memory_bytes=10 ** 13) == 10_000_000
+
+
+def test_genetic_map_helpers(tmp_path):
+    m = tmp_path / "map.txt"
+    m.write_text("pos\tMap(cM)\n0\t0.0\n1000000\t1.0\n2000000\t3.0\n")
+    pos = np.array([0, 500_000, 1_000_000, 1_500_000, 2_000_000])
+    gen = moments_ld._interpolate_genetic_distances(pos, str(m))
+    np.testing.assert_allclose(gen, [0.0, 0.005, 0.01, 0.02, 0.03])
+    # slowest rate 1e-8 / bp: 1e-3 M -> 1e5 bp x 1.1
+    assert abs(moments_ld._max_bp_for_r_dist(pos, gen, 1e-3) - 110_000.0) < 1e-6
+    assert moments_ld._max_bp_for_r_dist(pos, gen, 10.0) == 2_000_000.0
