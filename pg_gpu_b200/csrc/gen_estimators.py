@@ -602,7 +602,7 @@ def emit_geno(P):
         if n in feats:
             L.append(f"    x.{n} = {_cexpr(e)};")
     L.append("}")
-    L.append("template <typename T>")
+    L.append("template <typename T, int S = 1>")
     L.append(f"LDK_DEV void geno_stats_P{P}(const GenoFeat<T>* f, T* acc) {{")
     for ci, (case, args) in enumerate(calls):
         L.append(f"    const T v{ci} = {_cexpr(geno_call_expr(case, args))};  // {case}{args}")
@@ -615,7 +615,7 @@ def emit_geno(P):
             sw = _fmt_weight(w)
             body = " + ".join(vs)
             parts.append(body if sw is None else f"T({sw}) * ({body})")
-        L.append(f"    acc[{si}] += {' + '.join(parts)};  // {name}")
+        L.append(f"    acc[{si} * S] += {' + '.join(parts)};  // {name}")
     L.append("}")
     return "\n".join(L)
 
@@ -678,7 +678,7 @@ def emit_hap(P):
         if n in feats:
             L.append(f"    x.{n} = {_cexpr(e)};")
     L.append("}")
-    L.append("template <typename T>")
+    L.append("template <typename T, int S = 1>")
     L.append(f"LDK_DEV void hap_stats_P{P}(const HapFeat<T>* f, T* acc) {{")
     for ci, (case, args) in enumerate(calls):
         L.append(f"    const T v{ci} = {_cexpr(hap_call_expr(case, args))};  // {case}{args}")
@@ -691,7 +691,7 @@ def emit_hap(P):
             sw = _fmt_weight(w)
             body = " + ".join(vs)
             parts.append(body if sw is None else f"T({sw}) * ({body})")
-        L.append(f"    acc[{si}] += {' + '.join(parts)};  // {name}")
+        L.append(f"    acc[{si} * S] += {' + '.join(parts)};  // {name}")
     L.append("}")
     return "\n".join(L)
 
@@ -741,19 +741,19 @@ LDK_DEV void geno_features(GenoFeat<T>& x) {
     else if constexpr (P == 3) geno_features_P3<T>(x);
     else geno_features_P4<T>(x);
 }
-template <typename T, int P>
+template <typename T, int P, int S = 1>
 LDK_DEV void geno_stats(const GenoFeat<T>* f, T* acc) {
-    if constexpr (P == 1) geno_stats_P1<T>(f, acc);
-    else if constexpr (P == 2) geno_stats_P2<T>(f, acc);
-    else if constexpr (P == 3) geno_stats_P3<T>(f, acc);
-    else geno_stats_P4<T>(f, acc);
+    if constexpr (P == 1) geno_stats_P1<T, S>(f, acc);
+    else if constexpr (P == 2) geno_stats_P2<T, S>(f, acc);
+    else if constexpr (P == 3) geno_stats_P3<T, S>(f, acc);
+    else geno_stats_P4<T, S>(f, acc);
 }
-template <typename T, int P>
+template <typename T, int P, int S = 1>
 LDK_DEV void hap_stats(const HapFeat<T>* f, T* acc) {
-    if constexpr (P == 1) hap_stats_P1<T>(f, acc);
-    else if constexpr (P == 2) hap_stats_P2<T>(f, acc);
-    else if constexpr (P == 3) hap_stats_P3<T>(f, acc);
-    else hap_stats_P4<T>(f, acc);
+    if constexpr (P == 1) hap_stats_P1<T, S>(f, acc);
+    else if constexpr (P == 2) hap_stats_P2<T, S>(f, acc);
+    else if constexpr (P == 3) hap_stats_P3<T, S>(f, acc);
+    else hap_stats_P4<T, S>(f, acc);
 }
 """)
     text = "\n".join(parts)

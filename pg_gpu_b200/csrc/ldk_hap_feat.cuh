@@ -61,11 +61,23 @@ LDK_DEV void hap_set_counts(HapFeat<T>& x, T c1, T c2, T c3, T c4) {
 
 // r^2 of one population from its counts; NaN-free form: returns false where the
 // reference returns NaN (pA qA pB qB == 0, haplotype_kernels.py:32-42).
+// 1/x in double: hardware reciprocal estimate refined by two Newton-Raphson steps
+// r <- r (2 - x r) (quadratic convergence from ~2^-20 to full precision).
+LDK_DEV double recip_newton(double x) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+}
+LDK_DEV float recip_newton(float x) { return 1.0f / x; }
+
 template <typename T>
 LDK_DEV bool hap_r2(const HapFeat<T>& x, T& r2) {
     const T den = (x.c1 + x.c2) * (x.c3 + x.c4) * ((x.c1 + x.c3) * (x.c2 + x.c4));
     if (!(den > T(0))) return false;
     const T e = x.c1 * x.c4 - x.c2 * x.c3;
-    r2 = (e * e) / den;
+    r2 = (e * e) * recip_newton(den);
     return true;
 }

@@ -52,6 +52,7 @@ cudaError_t launch_parse_tc(const ldk_parse_t* d, const ldk_parse_out_t* o, cons
                             const ParseShape& sh, int n_items, cudaStream_t s);
 int tc_rows_per_block(const ParseShape& sh);
 int tc_epilogue_warps();
+int tc_smem_accumulators();
 size_t tc_smem_bytes(const ParseShape& sh);
 
 cudaError_t launch_build_items(const Scratch& w, int n_windows, cudaStream_t s);

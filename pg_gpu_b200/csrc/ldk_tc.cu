@@ -160,6 +160,21 @@ LDK_DEV void tmem_ld16_wait(uint32_t taddr, uint32_t (&r)[16]) {
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
 }
+LDK_DEV void tmem_ld4(uint32_t taddr, uint32_t (&r)[4]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(taddr));
+}
+template <int P>
+LDK_DEV void tmem_wait4(uint32_t (&r)[P][4]) {
+#pragma unroll
+    for (int p = 0; p < P; ++p)
+        asm volatile("tcgen05.wait::ld.sync.aligned;"
+                     : "+r"(r[p][0]), "+r"(r[p][1]), "+r"(r[p][2]), "+r"(r[p][3])
+                     :
+                     : "memory");
+}
+
 template <int P>
 LDK_DEV void tmem_wait_regs(uint32_t (&r)[P][16]) {
 #pragma unroll
@@ -278,7 +293,7 @@ struct TcArgs {
     unsigned* status;
 };
 
-template <int P, typename T, int EPI>
+template <int P, typename T, int EPI, bool SACC>
 __global__ void __launch_bounds__(128 + 32 * EPI, 1)
     k_parse_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcArgs a) {
     using C = Cfg<P>;
@@ -290,6 +305,7 @@ __global__ void __launch_bounds__(128 + 32 * EPI, 1)
     double* sacc = reinterpret_cast<double*>(base + C::STAGES * C::STAGE_BYTES);      // [kSlots][nb][NS+1]
     unsigned* scnt = reinterpret_cast<unsigned*>(sacc + kSlots * nb * (NS + 1));        // [kSlots][nb][2]
     double4* rtab = reinterpret_cast<double4*>(scnt + ((kSlots * nb * 2 + 7) & ~7));     // [max_n + 1]
+    T* lacc = reinterpret_cast<T*>(rtab + a.max_n + 1);  // SACC: [EPI warps][NS + 1][32 lanes]
 
     __shared__ __align__(8) uint64_t full_bar[C::STAGES], empty_bar[C::STAGES], tfull[2], tempty[2];
     __shared__ uint32_t tmem_base_s;
@@ -404,7 +420,6 @@ __global__ void __launch_bounds__(128 + 32 * EPI, 1)
         const int L = quarter * 32 + lane;
         const int r = L >> 1, role = L & 1;
         const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
-        constexpr int CH = JPH / 8;  // chunks of 8 partners
         uint32_t tcount = 0;
         for (int item = blockIdx.x; item < a.n_items; item += gridDim.x) {
             if (epi_bar_or<EPI>(abort_s != 0)) break;
@@ -425,24 +440,53 @@ __global__ void __launch_bounds__(128 + 32 * EPI, 1)
                     row_ok = false;
                 }
             }
-            T acc[NS];
+            // Sums of the current bin: registers, or lane-private shared-memory slots
+            // (stride 32: lanes hit consecutive words) when registers are scarce.
+            constexpr int NA = SACC ? 1 : NS + 1;
+            constexpr int AS = SACC ? 32 : 1;
+            T racc[NA];
+            T* acc = SACC ? lacc + (size_t)e * (NS + 1) * 32 + lane : racc;
 #pragma unroll
-            for (int s = 0; s < NS; ++s) acc[s] = T(0);
-            T r2acc = T(0);
+            for (int s = 0; s <= NS; ++s) acc[s * AS] = T(0);
             unsigned np = 0, nr2 = 0;
             int cur = -1;
-            auto flush = [&]() {
-                if (cur >= 0 && cur < nb && np > 0) {
-                    double* dst = sacc + (slot * nb + cur) * (NS + 1);
+            // Warp-cooperative flush of the current bin's sums.  Lanes of a warp hold 16
+            // neighbouring rows and cross into a new bin at almost the same partner, so
+            // lanes flushing the same (block, bin) are summed with shuffles first and one
+            // leader adds the group's total to shared memory: no contended atomics.
+            // Every lane of the warp calls this (it shuffles with the full mask).
+            auto flush = [&](bool want) {
+                const int mykey = slot * nb + cur;
+                unsigned fm = __ballot_sync(0xffffffffu, want);
+                while (fm) {
+                    const int leader = __ffs(fm) - 1;
+                    const int key = __shfl_sync(0xffffffffu, mykey, leader);
+                    const bool mine = want && (mykey == key);
+                    double* dst = sacc + key * (NS + 1);
 #pragma unroll
-                    for (int s = 0; s < NS; ++s) atomicAdd(dst + s, (double)acc[s]);
-                    atomicAdd(dst + NS, (double)r2acc);
-                    atomicAdd(scnt + 2 * (slot * nb + cur), np);
-                    atomicAdd(scnt + 2 * (slot * nb + cur) + 1, nr2);
+                    for (int s = 0; s <= NS; ++s) {
+                        double x = mine ? (double)acc[s * AS] : 0.0;
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+                        if (lane == leader) atomicAdd(dst + s, x);  // other warps may share the bin
+                    }
+                    unsigned c0 = mine ? np : 0u, c1 = mine ? nr2 : 0u;
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        c0 += __shfl_xor_sync(0xffffffffu, c0, o);
+                        c1 += __shfl_xor_sync(0xffffffffu, c1, o);
+                    }
+                    if (lane == leader) {
+                        atomicAdd(scnt + 2 * key, c0);
+                        atomicAdd(scnt + 2 * key + 1, c1);
+                    }
+                    want = want && !mine;
+                    fm = __ballot_sync(0xffffffffu, want);
                 }
+            };
+            auto reset = [&]() {
 #pragma unroll
-                for (int s = 0; s < NS; ++s) acc[s] = T(0);
-                r2acc = T(0);
+                for (int s = 0; s <= NS; ++s) acc[s * AS] = T(0);
                 np = nr2 = 0;
             };
             bool ok = true;
@@ -451,59 +495,64 @@ __global__ void __launch_bounds__(128 + 32 * EPI, 1)
                 if (!mbar_wait(&tfull[buf], tph, &abort_s, a.status)) { ok = false; break; }
                 tc_fence_after();
                 const int j0 = row0 + t * C::NJ;
+                // Two partners per step: 4 TMEM columns per population, indexed with
+                // constants only so the counts stay in registers.
 #pragma unroll 1
-                for (int ch = 0; ch < CH; ++ch) {
-                    uint32_t v[P][16];
-                    const uint32_t col = buf * C::COLS + half * 2 * JPH + ch * 16;
+                for (int q = 0; q < JPH / 2; ++q) {
+                    uint32_t v[P][4];
+                    const uint32_t col = buf * C::COLS + half * 2 * JPH + q * 4;
 #pragma unroll
-                    for (int p = 0; p < P; ++p) tmem_ld16_wait(tmem + lane_base + col + p * C::N, v[p]);
-                    tmem_wait_regs<P>(v);
-                    if (ch == CH - 1) {
+                    for (int p = 0; p < P; ++p) tmem_ld4(tmem + lane_base + col + p * C::N, v[p]);
+                    tmem_wait4<P>(v);
+                    if (q == JPH / 2 - 1) {
                         tc_fence_before();
                         __syncwarp();
                         if (lane == 0) mbar_arrive(&tempty[buf]);
                     }
-#pragma unroll 1
-                    for (int tt = 0; tt < 4; ++tt) {
+                    {
                         HapFeat<T> f[P];
                         int nval[P];
 #pragma unroll
                         for (int p = 0; p < P; ++p) {
-                            // lane 2r: (hh, hv) of partners 2tt, 2tt+1; lane 2r+1: (vh, vv)
-                            const uint32_t sx = role ? v[p][4 * tt + 0] : v[p][4 * tt + 2];
-                            const uint32_t sy = role ? v[p][4 * tt + 1] : v[p][4 * tt + 3];
+                            // lane 2r: (hh, hv) of partners 2q, 2q+1; lane 2r+1: (vh, vv)
+                            const uint32_t sx = role ? v[p][0] : v[p][2];
+                            const uint32_t sy = role ? v[p][1] : v[p][3];
                             const uint32_t rx = __shfl_xor_sync(0xffffffffu, sx, 1);
                             const uint32_t ry = __shfl_xor_sync(0xffffffffu, sy, 1);
                             int hh, hv, vh, vv;
-                            if (role == 0) { hh = (int)v[p][4 * tt]; hv = (int)v[p][4 * tt + 1]; vh = (int)rx; vv = (int)ry; }
-                            else { vh = (int)v[p][4 * tt + 2]; vv = (int)v[p][4 * tt + 3]; hh = (int)rx; hv = (int)ry; }
+                            if (role == 0) { hh = (int)v[p][0]; hv = (int)v[p][1]; vh = (int)rx; vv = (int)ry; }
+                            else { vh = (int)v[p][2]; vv = (int)v[p][3]; hh = (int)rx; hv = (int)ry; }
                             hap_set_counts(f[p], T(hh), T(hv - hh), T(vh - hh), T(vv - hv - vh + hh));
                             nval[p] = vv;
                         }
-                        const int jj = half * JPH + ch * 8 + 2 * tt + role;
+                        const int jj = half * JPH + 2 * q + role;
                         const int j = j0 + jj;
-                        if (row_ok && j > i && j < my_jmax) {
-                            const int b = bin_advance(sedges, nb, cur, fabs(a.coord[j] - ci));
-                            if (b != cur) {
-                                flush();
-                                cur = b;
-                            }
+                        const bool valid = row_ok && j > i && j < my_jmax;
+                        const int b = valid ? bin_advance(sedges, nb, cur, fabs(a.coord[j] - ci)) : cur;
+                        const bool change = b != cur;
+                        const bool want = change && cur >= 0 && cur < nb && np > 0;
+                        if (__any_sync(0xffffffffu, want)) flush(want);
+                        if (change) {
+                            reset();
+                            cur = b;
+                        }
+                        if (valid) {
                             if (b >= 0 && b < nb) {
 #pragma unroll
                                 for (int p = 0; p < P; ++p) {
                                     hap_features<T, P>(f[p]);
                                     hap_reciprocals_from(f[p], rtab[nval[p]]);
                                 }
-                                hap_stats<T, P>(f, acc);
+                                hap_stats<T, P, AS>(f, acc);
                                 T r2;
-                                if (hap_r2(f[0], r2)) { r2acc += r2; ++nr2; }
+                                if (hap_r2(f[0], r2)) { acc[NS * AS] += r2; ++nr2; }
                                 ++np;
                             }
                         }
                     }
                 }
             }
-            flush();
+            flush(cur >= 0 && cur < nb && np > 0);
             (void)ok;
             // stage -> global, once per row block
             epi_bar<EPI>();
@@ -572,15 +621,25 @@ bool make_map(CUtensorMap* m, const uint8_t* planes, int64_t n_var, int ktot, in
 }
 
 template <int P>
-size_t smem_bytes_t(int nb, int max_n) {
+size_t smem_bytes_t(int nb, int max_n, size_t lane_acc_bytes = 0) {
     using C = Cfg<P>;
     return 1024 + (size_t)C::STAGES * C::STAGE_BYTES + (size_t)kSlots * nb * (C::NS + 1) * sizeof(double) +
-           (size_t)((kSlots * nb * 2 + 7) & ~7) * sizeof(unsigned) + (size_t)(max_n + 1) * sizeof(double4) + 32;
+           (size_t)((kSlots * nb * 2 + 7) & ~7) * sizeof(unsigned) + (size_t)(max_n + 1) * sizeof(double4) + 32 +
+           lane_acc_bytes;
 }
 
 }  // namespace
 
 int tc_rows_per_block(const ParseShape&) { return kRows; }
+
+// Per-lane bin sums in shared memory (LDK_TC_SMEM_ACC=1) or registers (default).
+int tc_smem_accumulators() {
+    static int v = [] {
+        const char* e = getenv("LDK_TC_SMEM_ACC");
+        return (e && atoi(e) == 1) ? 1 : 0;
+    }();
+    return v;
+}
 
 // Epilogue width of the tensor-core kernel: 4 warps unless LDK_TC_EPI_WARPS=8.
 int tc_epilogue_warps() {
@@ -620,7 +679,7 @@ cudaError_t launch_prep_planes(const ldk_parse_t* d, const Scratch& w, const Par
     return cudaGetLastError();
 }
 
-template <int P, typename T, int EPI>
+template <int P, typename T, int EPI, bool SACC>
 static cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w,
                                      const ParseShape& sh, int n_items, cudaStream_t s) {
     using C = Cfg<P>;
@@ -646,14 +705,16 @@ static cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t
     a.status = w.status;
     // at least half of an SM's shared memory, so that one CTA (holding all 512 TMEM
     // columns) runs per SM
-    size_t smem = smem_bytes_t<P>(d->n_bins, sh.max_n);
+    const size_t lane_acc = SACC ? (size_t)EPI * (C::NS + 1) * 32 * sizeof(T) : 0;
+    size_t smem = smem_bytes_t<P>(d->n_bins, sh.max_n, lane_acc);
     if (smem < kMinSmem) smem = kMinSmem;
-    cudaError_t e = cudaFuncSetAttribute(k_parse_tc<P, T, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
+    cudaError_t e = cudaFuncSetAttribute(k_parse_tc<P, T, EPI, SACC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     if (EPI == 8) {
         // the setmaxnreg split inside the kernel assumes exactly 168 registers per thread
         cudaFuncAttributes fa;
-        if (cudaFuncGetAttributes(&fa, k_parse_tc<P, T, EPI>) != cudaSuccess || fa.numRegs != 168)
+        if (cudaFuncGetAttributes(&fa, k_parse_tc<P, T, EPI, SACC>) != cudaSuccess || fa.numRegs != 168)
             return cudaErrorInvalidConfiguration;
     }
     int dev = 0, sms = 148;
@@ -661,7 +722,7 @@ static cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (n_items == 0) return cudaSuccess;
     const int grid = n_items < sms ? n_items : sms;
-    k_parse_tc<P, T, EPI><<<grid, 128 + 32 * EPI, smem, s>>>(mA, mB, a);
+    k_parse_tc<P, T, EPI, SACC><<<grid, 128 + 32 * EPI, smem, s>>>(mA, mB, a);
     return cudaGetLastError();
 }
 
@@ -669,12 +730,16 @@ cudaError_t launch_parse_tc(const ldk_parse_t* d, const ldk_parse_out_t* o, cons
                             const ParseShape& sh, int n_items, cudaStream_t s) {
     const bool f32 = d->method == LDK_METHOD_TC_FP32;
     const bool wide = tc_epilogue_warps() == 8;
-#define LDK_TC_CASE(PP)                                                                       \
-    case PP:                                                                                  \
-        if (f32) return wide ? launch_parse_tc_p<PP, float, 8>(d, o, w, sh, n_items, s)       \
-                             : launch_parse_tc_p<PP, float, 4>(d, o, w, sh, n_items, s);      \
-        return wide ? launch_parse_tc_p<PP, double, 8>(d, o, w, sh, n_items, s)               \
-                    : launch_parse_tc_p<PP, double, 4>(d, o, w, sh, n_items, s);
+    const bool sacc = tc_smem_accumulators() && sh.P <= 3;
+#define LDK_TC_ONE(PP, TT)                                                                          \
+    if (wide) return sacc ? launch_parse_tc_p<PP, TT, 8, true>(d, o, w, sh, n_items, s)             \
+                          : launch_parse_tc_p<PP, TT, 8, false>(d, o, w, sh, n_items, s);           \
+    return sacc ? launch_parse_tc_p<PP, TT, 4, true>(d, o, w, sh, n_items, s)                       \
+                : launch_parse_tc_p<PP, TT, 4, false>(d, o, w, sh, n_items, s);
+#define LDK_TC_CASE(PP)                                                                             \
+    case PP:                                                                                        \
+        if (f32) { LDK_TC_ONE(PP, float) }                                                          \
+        LDK_TC_ONE(PP, double)
     switch (sh.P) {
         LDK_TC_CASE(1)
         LDK_TC_CASE(2)
@@ -682,6 +747,7 @@ cudaError_t launch_parse_tc(const ldk_parse_t* d, const ldk_parse_out_t* o, cons
         LDK_TC_CASE(4)
         default: return cudaErrorInvalidValue;
     }
+#undef LDK_TC_ONE
 #undef LDK_TC_CASE
 }
 
