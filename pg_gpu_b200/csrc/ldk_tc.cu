@@ -19,13 +19,16 @@
 // Warp roles (one CTA per SM, persistent over row blocks):
 //   warp 0     TMA producer (A: row block, B: 32..128 partner SNPs, per 128-byte K chunk)
 //   warp 1     TMEM allocator and single-thread MMA issuer, double-buffered accumulators
-//   warps 2-9  epilogue: tcgen05.ld the counts, swap halves between lane pairs, evaluate
-//              the FP32 estimators, sum per distance bin in registers (bins are monotone
-//              in j for a fixed i), stage per-bin FP64 sums in shared memory, add them to
-//              the per-bootstrap-block FP64 outputs once per row block.
+//   warps 4-7  epilogue, one per TMEM lane quarter: tcgen05.ld the counts, swap halves
+//              between lane pairs, evaluate the estimators (FP64, or FP32 for
+//              LDK_METHOD_TC_FP32), sum per distance bin in registers (bins are monotone
+//              in j for a fixed i), flush each finished bin run into a per-warp FP64
+//              staging copy in shared memory, and add the staged sums to the
+//              per-bootstrap-block FP64 outputs once per row block.
 // Every wait is bounded (LDK_DEVERR_TIMEOUT) so a fault cannot hang the GPU.
 #include <cuda.h>
 #include <cudaTypedefs.h>
+#include <math_constants.h>
 
 #include <cstdlib>
 #include <mutex>
@@ -39,12 +42,12 @@ namespace {
 
 constexpr int kRows = 64;               // SNPs per row block (M = 128 = 64 x {h, v})
 constexpr int kKChunk = 128;            // K bytes per TMA box / swizzle row
-// epilogue warps: 4 (one per TMEM lane quarter, up to 255 registers) or 8 (two per
-// quarter, each covering half of the partner columns, up to 192 registers)
+constexpr int kEpi = 4;                 // epilogue warps, one per TMEM lane quarter
 constexpr int kSlots = 2;               // bootstrap blocks staged per row block
 constexpr int kTmemCols = 512;
 constexpr uint64_t kTimeoutNs = 5000000000ull;  // 5 s per wait
 constexpr size_t kMinSmem = 116 * 1024;
+constexpr size_t kMaxSmem = 227 * 1024;
 
 template <int P>
 struct Cfg {
@@ -293,8 +296,8 @@ struct TcArgs {
     unsigned* status;
 };
 
-template <int P, typename T, int EPI, bool SACC>
-__global__ void __launch_bounds__(128 + 32 * EPI, 1)
+template <int P, typename T, bool PRIV>
+__global__ void __launch_bounds__(128 + 32 * kEpi, 1)
     k_parse_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcArgs a) {
     using C = Cfg<P>;
     constexpr int NS = C::NS;
@@ -302,10 +305,10 @@ __global__ void __launch_bounds__(128 + 32 * EPI, 1)
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int nb = a.edges.n_bins;
     unsigned char* stages = base;
-    double* sacc = reinterpret_cast<double*>(base + C::STAGES * C::STAGE_BYTES);      // [kSlots][nb][NS+1]
-    unsigned* scnt = reinterpret_cast<unsigned*>(sacc + kSlots * nb * (NS + 1));        // [kSlots][nb][2]
-    double4* rtab = reinterpret_cast<double4*>(scnt + ((kSlots * nb * 2 + 7) & ~7));     // [max_n + 1]
-    T* lacc = reinterpret_cast<T*>(rtab + a.max_n + 1);  // SACC: [EPI warps][NS + 1][32 lanes]
+    constexpr int NCOPY = PRIV ? kEpi : 1;  // staging copies: one per epilogue warp, or shared
+    double* sacc = reinterpret_cast<double*>(base + C::STAGES * C::STAGE_BYTES);  // [NCOPY][kSlots][nb][NS+1]
+    unsigned* scnt = reinterpret_cast<unsigned*>(sacc + NCOPY * kSlots * nb * (NS + 1));  // [NCOPY][kSlots][nb][2]
+    double4* rtab = reinterpret_cast<double4*>(scnt + ((NCOPY * kSlots * nb * 2 + 7) & ~7));  // [max_n + 1]
 
     __shared__ __align__(8) uint64_t full_bar[C::STAGES], empty_bar[C::STAGES], tfull[2], tempty[2];
     __shared__ uint32_t tmem_base_s;
@@ -320,14 +323,14 @@ __global__ void __launch_bounds__(128 + 32 * EPI, 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], EPI);
+            mbar_init(&tempty[b], kEpi);
         }
         abort_s = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int b = threadIdx.x; b <= nb; b += blockDim.x) sedges[b] = a.edges.e[b];
-    for (int idx = threadIdx.x; idx < kSlots * nb * (NS + 1); idx += blockDim.x) sacc[idx] = 0.0;
-    for (int idx = threadIdx.x; idx < kSlots * nb * 2; idx += blockDim.x) scnt[idx] = 0u;
+    for (int idx = threadIdx.x; idx < NCOPY * kSlots * nb * (NS + 1); idx += blockDim.x) sacc[idx] = 0.0;
+    for (int idx = threadIdx.x; idx < NCOPY * kSlots * nb * 2; idx += blockDim.x) scnt[idx] = 0u;
     for (int idx = threadIdx.x; idx <= a.max_n; idx += blockDim.x) rtab[idx] = recip_entry(idx);
     if (warp == 1) {
         tmem_alloc(&tmem_base_s, kTmemCols);
@@ -337,14 +340,6 @@ __global__ void __launch_bounds__(128 + 32 * EPI, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_base_s;
-    if constexpr (EPI == 8) {
-        // Rebalance the register file before any role waits on another: the control
-        // warpgroup gives up registers first (4 x 32 x 56 + 8 x 32 x 224 = 384 x 168, the
-        // launch allocation checked on the host), the epilogue warpgroups take them.
-        if (warp < 4) asm volatile("setmaxnreg.dec.sync.aligned.u32 56;");
-        else asm volatile("setmaxnreg.inc.sync.aligned.u32 224;");
-    }
-
     if (warp == 0) {
         // ------------------------------------------------------------- TMA producer
         if (lane == 0) {
@@ -413,16 +408,16 @@ __global__ void __launch_bounds__(128 + 32 * EPI, 1)
     }
     if (warp >= 4) {
         // ------------------------------------------------------------- epilogue
-        constexpr int HALVES = EPI / 4;
-        constexpr int JPH = C::NJ / HALVES;  // partners per thread group
         const int e = warp - 4;
-        const int quarter = warp & 3, half = e >> 2;
-        const int L = quarter * 32 + lane;
+        const int L = (warp & 3) * 32 + lane;
         const int r = L >> 1, role = L & 1;
-        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+        const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+        const int stage_n = kSlots * nb * (NS + 1);
+        double* my_sacc = sacc + (PRIV ? e * stage_n : 0);
+        unsigned* my_scnt = scnt + (PRIV ? e * kSlots * nb * 2 : 0);
         uint32_t tcount = 0;
         for (int item = blockIdx.x; item < a.n_items; item += gridDim.x) {
-            if (epi_bar_or<EPI>(abort_s != 0)) break;
+            if (epi_bar_or<kEpi>(abort_s != 0)) break;
             const int row0 = a.items[2 * item], row1 = a.items[2 * item + 1];
             const int jend = a.jmax[row1 - 1];
             const int n_jt = jend > row0 + 1 ? (jend - row0 + C::NJ - 1) / C::NJ : 0;
@@ -440,146 +435,157 @@ __global__ void __launch_bounds__(128 + 32 * EPI, 1)
                     row_ok = false;
                 }
             }
-            // Sums of the current bin: registers, or lane-private shared-memory slots
-            // (stride 32: lanes hit consecutive words) when registers are scarce.
-            constexpr int NA = SACC ? 1 : NS + 1;
-            constexpr int AS = SACC ? 32 : 1;
-            T racc[NA];
-            T* acc = SACC ? lacc + (size_t)e * (NS + 1) * 32 + lane : racc;
+            // Sums of the current bin live in registers.  Partners come in increasing j,
+            // so the distance to them never decreases and each (row, bin) run is flushed
+            // to shared memory once, when the lane's next partner falls past the bin's
+            // upper edge (held in `nxt`).
+            T acc[NS + 1];
 #pragma unroll
-            for (int s = 0; s <= NS; ++s) acc[s * AS] = T(0);
+            for (int s = 0; s <= NS; ++s) acc[s] = T(0);
             unsigned np = 0, nr2 = 0;
             int cur = -1;
-            // Warp-cooperative flush of the current bin's sums.  Lanes of a warp hold 16
-            // neighbouring rows and cross into a new bin at almost the same partner, so
-            // lanes flushing the same (block, bin) are summed with shuffles first and one
-            // leader adds the group's total to shared memory: no contended atomics.
-            // Every lane of the warp calls this (it shuffles with the full mask).
+            double nxt = sedges[0];
+            // Adds the flushing lanes' sums into shared memory.  With PRIV every epilogue
+            // warp owns its staging copy and the lanes of one warp that flush the same
+            // (block, bin) take turns (one lane per key per round), so plain adds suffice;
+            // otherwise the copy is shared by the warps and the adds are atomic.  Called by
+            // all 32 lanes.
             auto flush = [&](bool want) {
-                const int mykey = slot * nb + cur;
-                unsigned fm = __ballot_sync(0xffffffffu, want);
-                while (fm) {
-                    const int leader = __ffs(fm) - 1;
-                    const int key = __shfl_sync(0xffffffffu, mykey, leader);
-                    const bool mine = want && (mykey == key);
-                    double* dst = sacc + key * (NS + 1);
+                const int key = slot * nb + cur;
+                if constexpr (PRIV) {
+                    const unsigned grp = __match_any_sync(0xffffffffu, want ? key : -1);
+                    const int rank = __popc(grp & ((1u << lane) - 1u));
+                    const int rounds = (int)__reduce_max_sync(0xffffffffu, want ? (unsigned)__popc(grp) : 0u);
+                    double* dst = my_sacc + key * (NS + 1);
+                    for (int rr = 0; rr < rounds; ++rr) {
+                        if (want && rank == rr) {
 #pragma unroll
-                    for (int s = 0; s <= NS; ++s) {
-                        double x = mine ? (double)acc[s * AS] : 0.0;
+                            for (int s = 0; s <= NS; ++s) dst[s] += (double)acc[s];
+                            my_scnt[2 * key] += np;
+                            my_scnt[2 * key + 1] += nr2;
+                        }
+                        __syncwarp();
+                    }
+                } else if (want) {
+                    double* dst = my_sacc + key * (NS + 1);
 #pragma unroll
-                        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-                        if (lane == leader) atomicAdd(dst + s, x);  // other warps may share the bin
-                    }
-                    unsigned c0 = mine ? np : 0u, c1 = mine ? nr2 : 0u;
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) {
-                        c0 += __shfl_xor_sync(0xffffffffu, c0, o);
-                        c1 += __shfl_xor_sync(0xffffffffu, c1, o);
-                    }
-                    if (lane == leader) {
-                        atomicAdd(scnt + 2 * key, c0);
-                        atomicAdd(scnt + 2 * key + 1, c1);
-                    }
-                    want = want && !mine;
-                    fm = __ballot_sync(0xffffffffu, want);
+                    for (int s = 0; s <= NS; ++s) atomicAdd(dst + s, (double)acc[s]);
+                    atomicAdd(my_scnt + 2 * key, np);
+                    atomicAdd(my_scnt + 2 * key + 1, nr2);
                 }
-            };
-            auto reset = [&]() {
-#pragma unroll
-                for (int s = 0; s <= NS; ++s) acc[s * AS] = T(0);
-                np = nr2 = 0;
             };
             bool ok = true;
             for (int t = 0; t < n_jt; ++t, ++tcount) {
                 const uint32_t buf = tcount & 1u, tph = (tcount >> 1) & 1u;
+                const int j0 = row0 + t * C::NJ;
+                // partner coordinates of this tile, one per lane and register
+                double creg[C::NJ / 32];
+#pragma unroll
+                for (int k = 0; k < C::NJ / 32; ++k) {
+                    const int j = j0 + 32 * k + lane;
+                    creg[k] = j < jend ? a.coord[j] : 0.0;
+                }
                 if (!mbar_wait(&tfull[buf], tph, &abort_s, a.status)) { ok = false; break; }
                 tc_fence_after();
-                const int j0 = row0 + t * C::NJ;
                 // Two partners per step: 4 TMEM columns per population, indexed with
                 // constants only so the counts stay in registers.
 #pragma unroll 1
-                for (int q = 0; q < JPH / 2; ++q) {
+                for (int q = 0; q < C::NJ / 2; ++q) {
                     uint32_t v[P][4];
-                    const uint32_t col = buf * C::COLS + half * 2 * JPH + q * 4;
+                    const uint32_t col = buf * C::COLS + q * 4;
 #pragma unroll
                     for (int p = 0; p < P; ++p) tmem_ld4(tmem + lane_base + col + p * C::N, v[p]);
+                    const int jj = 2 * q + role;
+                    double csrc = creg[0];
+#pragma unroll
+                    for (int k = 1; k < C::NJ / 32; ++k)
+                        if ((q >> 4) == k) csrc = creg[k];
+                    const double cj = __shfl_sync(0xffffffffu, csrc, jj & 31);
                     tmem_wait4<P>(v);
-                    if (q == JPH / 2 - 1) {
+                    if (q == C::NJ / 2 - 1) {
                         tc_fence_before();
                         __syncwarp();
                         if (lane == 0) mbar_arrive(&tempty[buf]);
                     }
-                    {
-                        HapFeat<T> f[P];
-                        int nval[P];
+                    HapFeat<T> f[P];
+                    int nval[P];
+#pragma unroll
+                    for (int p = 0; p < P; ++p) {
+                        // lane 2r: (hh, hv) of partners 2q, 2q+1; lane 2r+1: (vh, vv)
+                        const uint32_t sx = role ? v[p][0] : v[p][2];
+                        const uint32_t sy = role ? v[p][1] : v[p][3];
+                        const uint32_t rx = __shfl_xor_sync(0xffffffffu, sx, 1);
+                        const uint32_t ry = __shfl_xor_sync(0xffffffffu, sy, 1);
+                        int hh, hv, vh, vv;
+                        if (role == 0) { hh = (int)v[p][0]; hv = (int)v[p][1]; vh = (int)rx; vv = (int)ry; }
+                        else { vh = (int)v[p][2]; vv = (int)v[p][3]; hh = (int)rx; hv = (int)ry; }
+                        hap_set_counts(f[p], T(hh), T(hv - hh), T(vh - hh), T(vv - hv - vh + hh));
+                        nval[p] = vv;
+                    }
+                    const int j = j0 + jj;
+                    const bool valid = row_ok && j > i && j < my_jmax;
+                    const double dist = fabs(cj - ci);
+                    const bool change = valid && dist >= nxt;
+                    const bool want = change && cur >= 0 && np > 0;
+                    if (__ballot_sync(0xffffffffu, want)) flush(want);
+                    if (change) {
+                        cur = bin_advance(sedges, nb, cur, dist);
+                        nxt = cur < nb ? sedges[cur + 1] : CUDART_INF;
+#pragma unroll
+                        for (int s = 0; s <= NS; ++s) acc[s] = T(0);
+                        np = nr2 = 0;
+                    }
+                    if (valid && cur >= 0 && cur < nb) {
 #pragma unroll
                         for (int p = 0; p < P; ++p) {
-                            // lane 2r: (hh, hv) of partners 2q, 2q+1; lane 2r+1: (vh, vv)
-                            const uint32_t sx = role ? v[p][0] : v[p][2];
-                            const uint32_t sy = role ? v[p][1] : v[p][3];
-                            const uint32_t rx = __shfl_xor_sync(0xffffffffu, sx, 1);
-                            const uint32_t ry = __shfl_xor_sync(0xffffffffu, sy, 1);
-                            int hh, hv, vh, vv;
-                            if (role == 0) { hh = (int)v[p][0]; hv = (int)v[p][1]; vh = (int)rx; vv = (int)ry; }
-                            else { vh = (int)v[p][2]; vv = (int)v[p][3]; hh = (int)rx; hv = (int)ry; }
-                            hap_set_counts(f[p], T(hh), T(hv - hh), T(vh - hh), T(vv - hv - vh + hh));
-                            nval[p] = vv;
+                            hap_features<T, P>(f[p]);
+                            hap_reciprocals_from(f[p], rtab[nval[p]]);
                         }
-                        const int jj = half * JPH + 2 * q + role;
-                        const int j = j0 + jj;
-                        const bool valid = row_ok && j > i && j < my_jmax;
-                        const int b = valid ? bin_advance(sedges, nb, cur, fabs(a.coord[j] - ci)) : cur;
-                        const bool change = b != cur;
-                        const bool want = change && cur >= 0 && cur < nb && np > 0;
-                        if (__any_sync(0xffffffffu, want)) flush(want);
-                        if (change) {
-                            reset();
-                            cur = b;
-                        }
-                        if (valid) {
-                            if (b >= 0 && b < nb) {
-#pragma unroll
-                                for (int p = 0; p < P; ++p) {
-                                    hap_features<T, P>(f[p]);
-                                    hap_reciprocals_from(f[p], rtab[nval[p]]);
-                                }
-                                hap_stats<T, P, AS>(f, acc);
-                                T r2;
-                                if (hap_r2(f[0], r2)) { acc[NS * AS] += r2; ++nr2; }
-                                ++np;
-                            }
-                        }
+                        hap_stats<T, P, 1>(f, acc);
+                        T r2;
+                        if (hap_r2(f[0], r2)) { acc[NS] += r2; ++nr2; }
+                        ++np;
                     }
                 }
             }
             flush(cur >= 0 && cur < nb && np > 0);
             (void)ok;
-            // stage -> global, once per row block
-            epi_bar<EPI>();
+            // staging -> global, once per row block
+            epi_bar<kEpi>();
             const int et = threadIdx.x - 128;
-            for (int idx = et; idx < kSlots * nb * (NS + 1); idx += 32 * EPI) {
+            for (int idx = et; idx < stage_n; idx += 32 * kEpi) {
+                double val = 0.0;
+#pragma unroll
+                for (int w = 0; w < (PRIV ? kEpi : 1); ++w) {
+                    val += sacc[w * stage_n + idx];
+                    sacc[w * stage_n + idx] = 0.0;
+                }
                 const int sl = idx / (nb * (NS + 1));
                 const int rem = idx % (nb * (NS + 1));
                 const int bb = rem / (NS + 1), s = rem % (NS + 1);
-                const double val = sacc[idx];
                 const int blk = blk0 + sl;
                 if (val != 0.0 && blk < a.n_blocks) {
                     if (s < NS) atomicAdd(&a.sums[((int64_t)blk * nb + bb) * NS + s], val);
                     else atomicAdd(&a.r2_sums[(int64_t)blk * nb + bb], val);
                 }
-                sacc[idx] = 0.0;
             }
-            for (int idx = et; idx < kSlots * nb; idx += 32 * EPI) {
+            for (int idx = et; idx < kSlots * nb; idx += 32 * kEpi) {
+                unsigned long long c0 = 0, c1 = 0;
+#pragma unroll
+                for (int w = 0; w < (PRIV ? kEpi : 1); ++w) {
+                    unsigned* sc = scnt + w * kSlots * nb * 2;
+                    c0 += sc[2 * idx];
+                    c1 += sc[2 * idx + 1];
+                    sc[2 * idx] = 0u;
+                    sc[2 * idx + 1] = 0u;
+                }
                 const int blk = blk0 + idx / nb, bb = idx % nb;
                 if (blk < a.n_blocks) {
-                    if (scnt[2 * idx]) atomicAdd(&a.pairs[(int64_t)blk * nb + bb], (unsigned long long)scnt[2 * idx]);
-                    if (scnt[2 * idx + 1])
-                        atomicAdd(&a.r2_counts[(int64_t)blk * nb + bb], (unsigned long long)scnt[2 * idx + 1]);
+                    if (c0) atomicAdd(&a.pairs[(int64_t)blk * nb + bb], c0);
+                    if (c1) atomicAdd(&a.r2_counts[(int64_t)blk * nb + bb], c1);
                 }
-                scnt[2 * idx] = 0u;
-                scnt[2 * idx + 1] = 0u;
             }
-            epi_bar<EPI>();
+            epi_bar<kEpi>();
         }
     }
     tc_fence_before();
@@ -621,41 +627,26 @@ bool make_map(CUtensorMap* m, const uint8_t* planes, int64_t n_var, int ktot, in
 }
 
 template <int P>
-size_t smem_bytes_t(int nb, int max_n, size_t lane_acc_bytes = 0) {
+size_t smem_bytes_t(int nb, int max_n, int ncopy) {
     using C = Cfg<P>;
-    return 1024 + (size_t)C::STAGES * C::STAGE_BYTES + (size_t)kSlots * nb * (C::NS + 1) * sizeof(double) +
-           (size_t)((kSlots * nb * 2 + 7) & ~7) * sizeof(unsigned) + (size_t)(max_n + 1) * sizeof(double4) + 32 +
-           lane_acc_bytes;
+    return 1024 + (size_t)C::STAGES * C::STAGE_BYTES + (size_t)ncopy * kSlots * nb * (C::NS + 1) * sizeof(double) +
+           (size_t)((ncopy * kSlots * nb * 2 + 7) & ~7) * sizeof(unsigned) + (size_t)(max_n + 1) * sizeof(double4) + 32;
 }
+
+// Per-warp staging copies when they fit next to the pipeline stages.
+template <int P>
+bool private_staging(int nb, int max_n) { return smem_bytes_t<P>(nb, max_n, kEpi) <= kMaxSmem; }
 
 }  // namespace
 
 int tc_rows_per_block(const ParseShape&) { return kRows; }
 
-// Per-lane bin sums in shared memory (LDK_TC_SMEM_ACC=1) or registers (default).
-int tc_smem_accumulators() {
-    static int v = [] {
-        const char* e = getenv("LDK_TC_SMEM_ACC");
-        return (e && atoi(e) == 1) ? 1 : 0;
-    }();
-    return v;
-}
-
-// Epilogue width of the tensor-core kernel: 4 warps unless LDK_TC_EPI_WARPS=8.
-int tc_epilogue_warps() {
-    static int v = [] {
-        const char* e = getenv("LDK_TC_EPI_WARPS");
-        return (e && atoi(e) == 8) ? 8 : 4;
-    }();
-    return v;
-}
-
 size_t tc_smem_bytes(const ParseShape& sh) {
     switch (sh.P) {
-        case 1: return smem_bytes_t<1>(sh.n_bins, sh.max_n);
-        case 2: return smem_bytes_t<2>(sh.n_bins, sh.max_n);
-        case 3: return smem_bytes_t<3>(sh.n_bins, sh.max_n);
-        default: return smem_bytes_t<4>(sh.n_bins, sh.max_n);
+        case 1: return smem_bytes_t<1>(sh.n_bins, sh.max_n, 1);
+        case 2: return smem_bytes_t<2>(sh.n_bins, sh.max_n, 1);
+        case 3: return smem_bytes_t<3>(sh.n_bins, sh.max_n, 1);
+        default: return smem_bytes_t<4>(sh.n_bins, sh.max_n, 1);
     }
 }
 
@@ -679,7 +670,7 @@ cudaError_t launch_prep_planes(const ldk_parse_t* d, const Scratch& w, const Par
     return cudaGetLastError();
 }
 
-template <int P, typename T, int EPI, bool SACC>
+template <int P, typename T, bool PRIV>
 static cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w,
                                      const ParseShape& sh, int n_items, cudaStream_t s) {
     using C = Cfg<P>;
@@ -705,37 +696,26 @@ static cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t
     a.status = w.status;
     // at least half of an SM's shared memory, so that one CTA (holding all 512 TMEM
     // columns) runs per SM
-    const size_t lane_acc = SACC ? (size_t)EPI * (C::NS + 1) * 32 * sizeof(T) : 0;
-    size_t smem = smem_bytes_t<P>(d->n_bins, sh.max_n, lane_acc);
+    size_t smem = smem_bytes_t<P>(d->n_bins, sh.max_n, PRIV ? kEpi : 1);
     if (smem < kMinSmem) smem = kMinSmem;
-    if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
-    cudaError_t e = cudaFuncSetAttribute(k_parse_tc<P, T, EPI, SACC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (smem > kMaxSmem) return cudaErrorInvalidConfiguration;
+    cudaError_t e = cudaFuncSetAttribute(k_parse_tc<P, T, PRIV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    if (EPI == 8) {
-        // the setmaxnreg split inside the kernel assumes exactly 168 registers per thread
-        cudaFuncAttributes fa;
-        if (cudaFuncGetAttributes(&fa, k_parse_tc<P, T, EPI, SACC>) != cudaSuccess || fa.numRegs != 168)
-            return cudaErrorInvalidConfiguration;
-    }
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (n_items == 0) return cudaSuccess;
     const int grid = n_items < sms ? n_items : sms;
-    k_parse_tc<P, T, EPI, SACC><<<grid, 128 + 32 * EPI, smem, s>>>(mA, mB, a);
+    k_parse_tc<P, T, PRIV><<<grid, 128 + 32 * kEpi, smem, s>>>(mA, mB, a);
     return cudaGetLastError();
 }
 
 cudaError_t launch_parse_tc(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w,
                             const ParseShape& sh, int n_items, cudaStream_t s) {
     const bool f32 = d->method == LDK_METHOD_TC_FP32;
-    const bool wide = tc_epilogue_warps() == 8;
-    const bool sacc = tc_smem_accumulators() && sh.P <= 3;
 #define LDK_TC_ONE(PP, TT)                                                                          \
-    if (wide) return sacc ? launch_parse_tc_p<PP, TT, 8, true>(d, o, w, sh, n_items, s)             \
-                          : launch_parse_tc_p<PP, TT, 8, false>(d, o, w, sh, n_items, s);           \
-    return sacc ? launch_parse_tc_p<PP, TT, 4, true>(d, o, w, sh, n_items, s)                       \
-                : launch_parse_tc_p<PP, TT, 4, false>(d, o, w, sh, n_items, s);
+    return private_staging<PP>(sh.n_bins, sh.max_n) ? launch_parse_tc_p<PP, TT, true>(d, o, w, sh, n_items, s) \
+                                                    : launch_parse_tc_p<PP, TT, false>(d, o, w, sh, n_items, s);
 #define LDK_TC_CASE(PP)                                                                             \
     case PP:                                                                                        \
         if (f32) { LDK_TC_ONE(PP, float) }                                                          \
