@@ -192,6 +192,7 @@ int ldk::parse_impl(const ldk_parse_t* d, const ldk_parse_out_t* out, void* work
     Scratch w;
     w.status = reinterpret_cast<unsigned*>(ws + L.status_off);
     w.row_counter = reinterpret_cast<int*>(ws + L.status_off + 64);
+    w.item_counter = reinterpret_cast<int*>(ws + L.status_off + 128);
     w.jmax = reinterpret_cast<int32_t*>(ws + L.jmax_off);
     w.win_off = reinterpret_cast<int64_t*>(ws + L.win_off);
     w.items = reinterpret_cast<int32_t*>(ws + L.items_off);

@@ -12,6 +12,7 @@ namespace ldk {
 struct Scratch {
     unsigned* status;      // device status word (LDK_DEVERR_* bits)
     int* row_counter;      // dynamic row-chunk counter of the plain parse
+    int* item_counter;     // dynamic row-block counter of the tensor-core parse
     int32_t* jmax;         // (n_var) exclusive end of each SNP's partner range
     int64_t* win_off;      // (n_windows + 1) window SNP offsets
     uint8_t* hv;           // TC path: (n_var, planes, Ktot) indicator planes

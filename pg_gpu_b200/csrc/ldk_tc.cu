@@ -44,6 +44,7 @@ constexpr int kRows = 64;               // SNPs per row block (M = 128 = 64 x {h
 constexpr int kKChunk = 128;            // K bytes per TMA box / swizzle row
 constexpr int kEpi = 4;                 // epilogue warps, one per TMEM lane quarter
 constexpr int kSlots = 2;               // bootstrap blocks staged per row block
+constexpr int kRing = 2;                // claimed row blocks in flight between the roles
 constexpr int kTmemCols = 512;
 constexpr uint64_t kTimeoutNs = 5000000000ull;  // 5 s per wait
 constexpr size_t kMinSmem = 116 * 1024;
@@ -285,6 +286,7 @@ struct TcArgs {
     int n_blocks;
     const int32_t* items;  // (n_items, 2): [row0, row1) row blocks
     int n_items;
+    int* item_counter;     // next unclaimed row block (zero at launch)
     int nkc;               // K chunks of 128 bytes
     int kofs[LDK_MAX_POPS + 1];
     int max_n;             // largest population (reciprocal table size - 1)
@@ -311,6 +313,8 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
     double4* rtab = reinterpret_cast<double4*>(scnt + ((NCOPY * kSlots * nb * 2 + 7) & ~7));  // [max_n + 1]
 
     __shared__ __align__(8) uint64_t full_bar[C::STAGES], empty_bar[C::STAGES], tfull[2], tempty[2];
+    __shared__ __align__(8) uint64_t ifull[kRing], iempty[kRing];
+    __shared__ volatile int ring[kRing];
     __shared__ uint32_t tmem_base_s;
     __shared__ volatile int abort_s;
     __shared__ double sedges[LDK_MAX_BINS + 1];
@@ -324,6 +328,10 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
         for (int b = 0; b < 2; ++b) {
             mbar_init(&tfull[b], 1);
             mbar_init(&tempty[b], kEpi);
+        }
+        for (int b = 0; b < kRing; ++b) {
+            mbar_init(&ifull[b], 1);
+            mbar_init(&iempty[b], 1 + kEpi);  // the MMA issuer and every epilogue warp
         }
         abort_s = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -345,7 +353,15 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
         if (lane == 0) {
             uint32_t it = 0;
             bool ok = true;
-            for (int item = blockIdx.x; item < a.n_items && ok; item += gridDim.x) {
+            for (uint32_t k = 0; ok; ++k) {
+                // claim the next row block and publish it to the MMA issuer and the epilogue
+                const int sl = k % kRing;
+                if (!mbar_wait(&iempty[sl], ((k / kRing) & 1u) ^ 1u, &abort_s, a.status)) { ok = false; break; }
+                int item = atomicAdd(a.item_counter, 1);
+                if (item >= a.n_items) item = -1;
+                ring[sl] = item;
+                mbar_arrive(&ifull[sl]);
+                if (item < 0) break;
                 const int row0 = a.items[2 * item], row1 = a.items[2 * item + 1];
                 const int jend = a.jmax[row1 - 1];
                 const int n_jt = jend > row0 + 1 ? (jend - row0 + C::NJ - 1) / C::NJ : 0;
@@ -371,7 +387,12 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
             constexpr uint32_t idesc = idesc_u8<C::N>();
             uint32_t it = 0, tcount = 0;
             bool ok = true;
-            for (int item = blockIdx.x; item < a.n_items && ok; item += gridDim.x) {
+            for (uint32_t k = 0; ok; ++k) {
+                const int sl = k % kRing;
+                if (!mbar_wait(&ifull[sl], (k / kRing) & 1u, &abort_s, a.status)) { ok = false; break; }
+                const int item = ring[sl];
+                mbar_arrive(&iempty[sl]);
+                if (item < 0) break;
                 const int row0 = a.items[2 * item], row1 = a.items[2 * item + 1];
                 const int jend = a.jmax[row1 - 1];
                 const int n_jt = jend > row0 + 1 ? (jend - row0 + C::NJ - 1) / C::NJ : 0;
@@ -416,8 +437,17 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
         double* my_sacc = sacc + (PRIV ? e * stage_n : 0);
         unsigned* my_scnt = scnt + (PRIV ? e * kSlots * nb * 2 : 0);
         uint32_t tcount = 0;
-        for (int item = blockIdx.x; item < a.n_items; item += gridDim.x) {
-            if (epi_bar_or<kEpi>(abort_s != 0)) break;
+        for (uint32_t k = 0;; ++k) {
+            const int sl = k % kRing;
+            int item = -1;
+            if (lane == 0) {
+                if (mbar_wait(&ifull[sl], (k / kRing) & 1u, &abort_s, a.status)) {
+                    item = ring[sl];
+                    mbar_arrive(&iempty[sl]);
+                }
+            }
+            item = __shfl_sync(0xffffffffu, item, 0);
+            if (epi_bar_or<kEpi>(abort_s != 0 || item < 0)) break;
             const int row0 = a.items[2 * item], row1 = a.items[2 * item + 1];
             const int jend = a.jmax[row1 - 1];
             const int n_jt = jend > row0 + 1 ? (jend - row0 + C::NJ - 1) / C::NJ : 0;
@@ -684,6 +714,7 @@ static cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t
     a.n_blocks = d->n_blocks;
     a.items = w.items;
     a.n_items = n_items;
+    a.item_counter = w.item_counter;
     a.nkc = sh.ktot / kKChunk;
     for (int p = 0; p <= LDK_MAX_POPS; ++p) a.kofs[p] = sh.kofs[p];
     a.max_n = sh.max_n;
