@@ -47,6 +47,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     from pg_gpu_b200.csrc import gen_estimators
 
     gen_estimators.check()
+    gen_estimators.fused_features_ok()
     gen_estimators.generate()
     sources = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
     deps = sources + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]

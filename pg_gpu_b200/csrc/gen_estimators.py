@@ -696,6 +696,241 @@ def emit_hap(P):
     return "\n".join(L)
 
 
+# ---------------------------------------------------------------------------
+# fused-path forms (tensor-core parse)
+# ---------------------------------------------------------------------------
+#
+# Statistic-level expressions over per-population *scaled* features (numerator factors
+# times their reciprocal denominators), written as one accumulate per product term so
+# that every term is a single FMA into its sum.  Every raw call's numerator is an
+# integer polynomial of the counts, exact in FP64 below 2^53, so regrouping it changes
+# only the final roundings.  Two identities shorten the pi2 cases:
+#   L_k = c_{5-k} ns - sigma_k E  (sigma = +1, -1, -1, +1), hence
+#   F_k = L_k - c_{5-k} = c_{5-k} (ns - 1) - sigma_k E, and the pi2(i,j,i,j) correction
+#   sum_k (Q_k^i c_{5-k}^j - c_k^i L_k^j) = X (1 - ns_i - ns_j) - (E_i s_j + E_j s_i),
+#   X = sum_k c_{5-k}^i c_k^j, symmetric in (i, j): pi2_ijij(i, j) = pi2_ijij(j, i).
+# ``check()`` verifies both symbolically.
+
+# (name, expression): x = f[p] (HapFeat), g = this population's scaled features
+FUSED_SCALED = [
+    ("Er2", "x.E * x.r2"),
+    ("Er2h", "0.5 * g.Er2"),
+    ("Er3h", "x.E * (0.5 * x.r3)"),
+    ("aEr3h", "x.a * g.Er3h"),
+    ("bEr3h", "x.b * g.Er3h"),
+    ("ar1", "x.a * x.r1"),
+    ("br1", "x.b * x.r1"),
+    ("Sr2", "(x.s + x.a * x.b) * x.r2"),
+    ("r3h", "0.5 * x.r3"),
+    ("T1r3h", "x.T1 * g.r3h"),
+    ("T2r3h", "x.T2 * g.r3h"),
+    ("pAr1", "x.pA * x.r1"),
+    ("qAr1", "x.qA * x.r1"),
+    ("pBr1", "x.pB * x.r1"),
+    ("qBr1", "x.qB * x.r1"),
+    ("r2h", "0.5 * x.r2"),
+    ("fAr2h", "x.fA * g.r2h"),
+    ("fBr2", "x.fB * x.r2"),
+    ("r2q", "0.25 * x.r2"),
+    ("fAr2q", "x.fA * g.r2q"),
+    ("fBr2q", "x.fB * g.r2q"),
+    ("r2e", "0.125 * x.r2"),
+    ("m1", "x.ns - 1"),
+    ("F1h", "(x.c4 * g.m1 - x.E) * g.r2e"),
+    ("F2h", "(x.c3 * g.m1 + x.E) * g.r2e"),
+    ("F3h", "(x.c2 * g.m1 + x.E) * g.r2e"),
+    ("F4h", "(x.c1 * g.m1 - x.E) * g.r2e"),
+]
+
+# features of HapFeat the fused forms read directly
+FUSED_BASE = ["c1", "c2", "c3", "c4", "ns", "pA", "qA", "pB", "qB", "E", "a", "b", "s", "fA", "fB",
+              "T1", "T2", "DDs", "DZs", "PIs"]
+
+
+def fused_plan(P):
+    """Per statistic, the list of (weight, case, args) with pi2_ijij merged over its
+    two argument orders."""
+    out = []
+    for name, cl in stat_specs(P):
+        terms = {}
+        for w, kind, p in cl:
+            case, args = canonical(kind, p)
+            if case == "pi2_ijij":
+                args = tuple(sorted(args))
+            terms[(case, args)] = terms.get((case, args), 0.0) + w
+        out.append((name, [(w, c, a) for (c, a), w in terms.items()]))
+    return out
+
+
+def fused_terms(case, args, w):
+    """Product terms (A, B) whose sum is w * call(case, args); A and B use f[p].name for
+    HapFeat fields and g{p}_name for scaled features."""
+    g = lambda p, n: f"g{p}_{n}"  # noqa: E731
+    f = lambda p, n: f"f[{p}].{n}"  # noqa: E731
+    need = {"dd1": 1.0, "dd2": 1.0, "dz_iii": 1.0, "dz_iij": 0.5, "dz_iji": 0.5, "dz_ijj": 1.0,
+            "dz_ijk": 0.5, "pi2_same": 1.0, "pi2_triple": 1.0, "pi2_iikk": 0.5, "pi2_iikl": 0.5,
+            "pi2_ijkk": 0.5, "pi2_alldiff": 0.5, "pi2_ijij": 1.0, "pi2_shared": 0.5}[case]
+    if w != need:
+        raise ValueError(f"weight {w} of {case}{args}: fused form assumes {need}")
+    if case == "dd1":
+        (i,) = args
+        return [(f(i, "DDs"), f(i, "r4"))]
+    if case == "dd2":
+        i, j = args
+        return [(g(i, "Er2"), g(j, "Er2"))]
+    if case == "dz_iii":
+        (i,) = args
+        return [(f(i, "DZs"), f(i, "r4"))]
+    if case == "dz_iij":
+        i, j = args
+        return [(g(i, "aEr3h"), g(j, "br1"))]
+    if case == "dz_iji":
+        i, j = args
+        return [(g(i, "bEr3h"), g(j, "ar1"))]
+    if case == "dz_ijj":
+        i, j = args
+        return [(g(i, "Er2"), g(j, "Sr2"))]
+    if case == "dz_ijk":
+        i, j, k = args
+        return [(g(i, "Er2h"), f"({g(j, 'ar1')} * {g(k, 'br1')})")]
+    if case == "pi2_same":
+        (i,) = args
+        return [(f(i, "PIs"), f(i, "r4"))]
+    if case == "pi2_triple":
+        t, s_ = args
+        return [(g(t, "T1r3h"), g(s_, "pBr1")), (g(t, "T2r3h"), g(s_, "qBr1"))]
+    if case == "pi2_iikk":
+        i, k = args
+        return [(g(i, "fAr2h"), g(k, "fBr2"))]
+    if case == "pi2_iikl":
+        i, k, l = args
+        return [(g(i, "fAr2q"), f"({g(k, 'pBr1')} * {g(l, 'qBr1')} + {g(k, 'qBr1')} * {g(l, 'pBr1')})")]
+    if case == "pi2_ijkk":
+        i, j, k = args
+        return [(g(k, "fBr2q"), f"({g(i, 'pAr1')} * {g(j, 'qAr1')} + {g(i, 'qAr1')} * {g(j, 'pAr1')})")]
+    if case == "pi2_alldiff":
+        i, j, k, l = args
+        return [(f"(0.125 * ({g(i, 'pAr1')} * {g(j, 'qAr1')} + {g(i, 'qAr1')} * {g(j, 'pAr1')}))",
+                 f"({g(k, 'pBr1')} * {g(l, 'qBr1')} + {g(k, 'qBr1')} * {g(l, 'pBr1')})")]
+    if case == "pi2_shared":
+        s_, a, b = args
+        return [(g(a, "pAr1"), f"({g(b, 'pBr1')} * {g(s_, 'F1h')} + {g(b, 'qBr1')} * {g(s_, 'F2h')})"),
+                (g(a, "qAr1"), f"({g(b, 'pBr1')} * {g(s_, 'F3h')} + {g(b, 'qBr1')} * {g(s_, 'F4h')})")]
+    if case == "pi2_ijij":
+        i, j = args
+        HA = f"({f(i, 'pA')} * {f(j, 'qA')} + {f(i, 'qA')} * {f(j, 'pA')})"
+        HB = f"({f(i, 'pB')} * {f(j, 'qB')} + {f(i, 'qB')} * {f(j, 'pB')})"
+        X = (f"({f(i, 'c4')} * {f(j, 'c1')} + {f(i, 'c3')} * {f(j, 'c2')} + {f(i, 'c2')} * {f(j, 'c3')}"
+             f" + {f(i, 'c1')} * {f(j, 'c4')})")
+        body = (f"({HA} * {HB} + {X} * (1 - {f(i, 'ns')} - {f(j, 'ns')})"
+                f" - ({f(i, 'E')} * {f(j, 's')} + {f(j, 'E')} * {f(i, 's')}))")
+        return [(f"({g(i, 'r2h')} * {g(j, 'r2h')})", body)]
+    raise ValueError(case)
+
+
+def _term_cost(A, B):
+    return 1 + sum(t.count("*") + t.count(" + ") + t.count(" - ") for t in (A, B))
+
+
+def fused_split(P):
+    """Split point K of the statistics into two contiguous halves of about equal cost."""
+    costs = [sum(_term_cost(A, B) for w, c, a in terms for A, B in fused_terms(c, a, w))
+             for _, terms in fused_plan(P)]
+    tot, run, best = sum(costs), 0, (None, 0)
+    for k in range(1, len(costs)):
+        run += costs[k - 1]
+        d = abs(2 * run - tot)
+        if best[0] is None or d < best[0]:
+            best = (d, k)
+    return best[1]
+
+
+def _scaled_closure(used):
+    """(p, name) scaled features needed by the used set, in definition order."""
+    defs = dict(FUSED_SCALED)
+    import re
+    need = set(used)
+    changed = True
+    while changed:
+        changed = False
+        for p, n in list(need):
+            for dep in re.findall(r"g\.(\w+)", defs[n]):
+                if (p, dep) not in need:
+                    need.add((p, dep))
+                    changed = True
+    order = [n for n, _ in FUSED_SCALED]
+    return sorted(need, key=lambda t: (t[0], order.index(t[1])))
+
+
+def emit_hap_fused(P):
+    """hap_fused_P{P}_{part}: part 0 = all statistics, 1 = [0, K), 2 = [K, NS)."""
+    import re
+    plan_ = fused_plan(P)
+    K = fused_split(P)
+    ranges = {0: (0, len(plan_)), 1: (0, K), 2: (K, len(plan_))}
+    L = [f"// P = {P}, fused path: statistics split at {K} of {len(plan_)}"]
+    for part, (lo, hi) in ranges.items():
+        lines, used = [], set()
+        for si in range(lo, hi):
+            name, terms = plan_[si]
+            for w, case, args in terms:
+                for A, B in fused_terms(case, args, w):
+                    for m in re.finditer(r"g(\d)_(\w+)", A + " " + B):
+                        used.add((int(m.group(1)), m.group(2)))
+                    lines.append(f"    acc[{si - lo}] += {_cexpr(A)} * {_cexpr(B)};  // {name}: {case}{args}")
+        defs = dict(FUSED_SCALED)
+        L.append("template <typename T>")
+        L.append(f"LDK_DEV void hap_fused_P{P}_{part}(const HapFeat<T>* f, T* acc) {{")
+        for p, n in _scaled_closure(used):
+            e = defs[n].replace("x.", f"f[{p}].")
+            e = re.sub(r"g\.(\w+)", lambda m: f"g{p}_{m.group(1)}", e)
+            L.append(f"    const T g{p}_{n} = {_cexpr(e)};")
+        L.extend(lines)
+        L.append("}")
+    return "\n".join(L)
+
+
+def fused_features_ok():
+    """Every HapFeat field the fused forms read is computed by hap_features_P*."""
+    import re
+    for P in (1, 2, 3, 4):
+        have = set(hap_features_needed(P)[0]) | {"c1", "c2", "c3", "c4", "ns", "n", "r1", "r2", "r3", "r4"}
+        text = " ".join(A + " " + B for _, terms in fused_plan(P) for w, c, a in terms for A, B in fused_terms(c, a, w))
+        text += " " + " ".join(e for _, e in FUSED_SCALED)
+        used = set(re.findall(r"f\[\d\]\.(\w+)", text))
+        scaled_used = {n for p_, n in _scaled_closure(
+            {(int(m.group(1)), m.group(2)) for m in re.finditer(r"g(\d)_(\w+)", text)})}
+        used |= {d for n, e in FUSED_SCALED if n in scaled_used for d in re.findall(r"x\.(\w+)", e)}
+        if not used <= have:
+            raise AssertionError(f"P={P}: fused forms read {sorted(used - have)} not computed")
+    return True
+
+
+def numpy_hap_fused(counts_list, n_list=None, part=0):
+    """Evaluate the fused forms with NumPy float64 (test helper); columns of the part."""
+    import re
+    import numpy as np
+    P = len(counts_list)
+    xs = _numpy_hap_feats(counts_list, n_list, all_features=True)
+    env = {}
+    for p, x in enumerate(xs):
+        for n, e in FUSED_SCALED:
+            g = _NS()
+            for k, v in env.items():
+                if k.startswith(f"g{p}_"):
+                    setattr(g, k[len(f"g{p}_"):], v)
+            env[f"g{p}_{n}"] = eval(e, {}, {"x": x, "g": g})
+    plan_ = fused_plan(P)
+    K = fused_split(P)
+    lo, hi = {0: (0, len(plan_)), 1: (0, K), 2: (K, len(plan_))}[part]
+    out = np.zeros((len(xs[0].c1), hi - lo))
+    for si in range(lo, hi):
+        for w, case, args in plan_[si][1]:
+            for A, B in fused_terms(case, args, w):
+                out[:, si - lo] += eval(A, {}, {"f": xs, **env}) * eval(B, {}, {"f": xs, **env})
+    return out
+
+
 def _cexpr(e):
     """Numeric literals as T(...) so float and double instantiations stay exact."""
     import re
@@ -707,6 +942,8 @@ HEADER = """// GENERATED by gen_estimators.py -- do not edit by hand.
 // Straight-line two-locus LD estimators for P = 1..4 populations (haplotype path).
 // Statistic order and averaging weights follow moments.LD (pg_gpu ld_pipeline.py:357-457);
 // raw-call algebra restates pg_gpu haplotype_kernels.py:69-304 in factored form.
+// hap_stats_P* evaluate every distinct raw call (plain kernel, raw-call entry points);
+// hap_fused_P* are the statistic-level forms of the tensor-core parse.
 #pragma once
 """
 
@@ -717,6 +954,9 @@ def generate(path=None):
     for P in (1, 2, 3, 4):
         parts.append(emit_hap(P))
         parts.append("")
+    for P in (1, 2, 3, 4):
+        parts.append(emit_hap_fused(P))
+        parts.append("")
     parts.append('#include "ldk_geno_feat.cuh"')
     for P in (1, 2, 3, 4):
         parts.append(emit_geno(P))
@@ -726,6 +966,10 @@ def generate(path=None):
     parts.append("template <int P> struct HapNStats;")
     for P in (1, 2, 3, 4):
         parts.append(f"template <> struct HapNStats<{P}> {{ static constexpr int value = {len(stat_specs(P))}; }};")
+    parts.append("// first statistic of the second half of the fused path's two-way split")
+    parts.append("template <int P> struct HapFusedSplit;")
+    for P in (1, 2, 3, 4):
+        parts.append(f"template <> struct HapFusedSplit<{P}> {{ static constexpr int value = {fused_split(P)}; }};")
     parts.append("""
 template <typename T, int P>
 LDK_DEV void hap_features(HapFeat<T>& x) {
@@ -747,6 +991,22 @@ LDK_DEV void geno_stats(const GenoFeat<T>* f, T* acc) {
     else if constexpr (P == 2) geno_stats_P2<T, S>(f, acc);
     else if constexpr (P == 3) geno_stats_P3<T, S>(f, acc);
     else geno_stats_P4<T, S>(f, acc);
+}
+// Fused-path statistics of part PART (0: all, 1: [0, split), 2: [split, NS)) added into
+// acc[0 ..) of that part.
+template <typename T, int P, int PART>
+LDK_DEV void hap_fused(const HapFeat<T>* f, T* acc) {
+#define LDK_FUSED_CASE(PP) \\
+    if constexpr (P == PP) { \\
+        if constexpr (PART == 0) hap_fused_P##PP##_0<T>(f, acc); \\
+        else if constexpr (PART == 1) hap_fused_P##PP##_1<T>(f, acc); \\
+        else hap_fused_P##PP##_2<T>(f, acc); \\
+    }
+    LDK_FUSED_CASE(1)
+    LDK_FUSED_CASE(2)
+    LDK_FUSED_CASE(3)
+    LDK_FUSED_CASE(4)
+#undef LDK_FUSED_CASE
 }
 template <typename T, int P, int S = 1>
 LDK_DEV void hap_stats(const HapFeat<T>* f, T* acc) {
@@ -771,11 +1031,10 @@ class _NS:
     pass
 
 
-def numpy_hap_stats(counts_list, n_list=None):
-    """Evaluate the generated expressions with NumPy float64 (test helper)."""
+def _numpy_hap_feats(counts_list, n_list=None, all_features=False):
     import numpy as np
     P = len(counts_list)
-    feats, _ = hap_features_needed(P)
+    feats = [n for n, _ in HAP_FEATURES] if all_features else hap_features_needed(P)[0]
     fs = []
     for p, c in enumerate(counts_list):
         c = np.asarray(c, dtype=np.float64)
@@ -795,7 +1054,14 @@ def numpy_hap_stats(counts_list, n_list=None):
             x.r3 = np.where(d3 > 0, 1 / np.where(d3 > 0, d3, 1), 0.0)
             x.r4 = np.where(d4 > 0, 1 / np.where(d4 > 0, d4, 1), 0.0)
         fs.append(x)
-    calls, stats = plan(P)
+    return fs
+
+
+def numpy_hap_stats(counts_list, n_list=None):
+    """Evaluate the generated expressions with NumPy float64 (test helper)."""
+    import numpy as np
+    fs = _numpy_hap_feats(counts_list, n_list)
+    calls, stats = plan(len(counts_list))
     vals = [eval(hap_call_expr(case, args), {}, {"f": fs}) for case, args in calls]
     out = np.zeros((len(fs[0].c1), len(stats)))
     for si, (_, terms) in enumerate(stats):
@@ -838,6 +1104,13 @@ def check():
     corr = (X.Q1 * b4 + X.Q2 * b3 + X.Q3 * b2 + X.Q4 * b1
             - (a1 * Y.L1 + a2 * Y.L2 + a3 * Y.L3 + a4 * Y.L4))
     assert sp.expand(ref_ijij - (HA * HB + corr) / 4) == 0
+    # fused path: the symmetric pi2(i,j,i,j) correction and F_k = L_k - c_{5-k}
+    Xs = a4 * b1 + a3 * b2 + a2 * b3 + a1 * b4
+    corr2 = Xs * (1 - X.ns - Y.ns) - (X.E * Y.s + Y.E * X.s)
+    assert sp.expand(corr - corr2) == 0
+    m1 = X.ns - 1
+    for Lk, ck, sig in ((X.L1, a4, 1), (X.L2, a3, -1), (X.L3, a2, -1), (X.L4, a1, 1)):
+        assert sp.expand((Lk - ck) - (ck * m1 - sig * X.E)) == 0
     # single-population numerators, haplotype_kernels.py:76, 102-104, 298-301
     c1, c2, c3, c4 = a
     assert sp.expand(X.DDs - (c1 * (c1 - 1) * c4 * (c4 - 1) + c2 * (c2 - 1) * c3 * (c3 - 1)
@@ -875,4 +1148,5 @@ def check():
 
 if __name__ == "__main__":
     check()
+    fused_features_ok()
     print(generate())

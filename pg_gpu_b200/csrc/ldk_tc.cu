@@ -571,7 +571,7 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
                             hap_features<T, P>(f[p]);
                             hap_reciprocals_from(f[p], rtab[nval[p]]);
                         }
-                        hap_stats<T, P, 1>(f, acc);
+                        hap_fused<T, P, 0>(f, acc);
                         T r2;
                         if (hap_r2(f[0], r2)) { acc[NS] += r2; ++nr2; }
                         ++np;
