@@ -363,7 +363,8 @@ def main():
 
     # ---- roofline of the dominant kernel
     pk_d, pk_kind = peaks()
-    int8_peak = 2.0 * pk_d["bf16_tflops"]
+    probe_i8, probe_f64 = _lib.probe_peaks()
+    int8_peak = probe_i8 / 1e12
     ops = algorithmic_int_ops_per_pair(w) * n_pairs
     achieved = ops / (k_ms / 1e3) / 1e12 if k_ms else None
     traffic = None
@@ -373,12 +374,24 @@ def main():
             tj = json.load(f)
         # captured on this full-size workload: bytes per launch as measured
         traffic = tj["dram_bytes_per_launch"] if tj.get("pairs") == n_pairs else None
+    fp64 = None
+    ifile = os.path.join(REPO, "profiles", "k_parse_tc_c4_fp64.json")
+    if os.path.exists(ifile) and args.config == 4 and args.method == "tc" and k_ms:
+        with open(ifile) as f:
+            fj = json.load(f)
+        per_pair = fj["fp64_thread_inst_per_pair"]
+        rate = per_pair * n_pairs / (k_ms / 1e3)
+        fp64 = {"inst_per_pair": per_pair, "inst_per_pair_source": "ncu, " + fj["workload"],
+                "achieved_inst_per_s": rate, "peak_fma_per_s": probe_f64, "frac": rate / probe_f64,
+                "peak_source": "ldk_probe_peaks in this run (8 FP64 FMA chains per thread, 16 warps per SM)"}
     roofline = {"bound": "tensor", "kernel": "k_parse_tc", "achieved": achieved, "peak": int8_peak,
                 "unit": "TOP/s (INT8, MAC=2)", "frac": (achieved / int8_peak) if achieved else None,
-                "peak_source": f"2 x {pk_kind} bf16 dense burst {pk_d['bf16_tflops']} TFLOP/s (derived)",
-                "traffic": traffic, "kernel_ms": k_ms,
+                "peak_source": "measured in this run: ldk_probe_peaks, back-to-back tcgen05 kind::i8 "
+                               "128x256x32 MMAs on every SM",
+                "peak_bf16x2_derived": 2.0 * pk_d["bf16_tflops"],
+                "traffic": traffic, "kernel_ms": k_ms, "fp64": fp64,
                 "note": "count stage algorithmic ops = 8 x sum(n_pop) per pair; the fused kernel is bound by "
-                        "its FP64 estimator epilogue, not by the tensor pipe"}
+                        "its FP64 estimator epilogue (see fp64), not by the tensor pipe"}
 
     if rank == 0:
         line = {

@@ -138,6 +138,13 @@ LDK_API int ldk_parse_noalloc(const ldk_parse_t* d, const ldk_parse_out_t* out, 
 LDK_API int ldk_profile(int enable);
 LDK_API double ldk_profile_last_kernel_ms(void);
 
+/* Measured peaks of the calling device, the denominators of the tensor-core parse's
+ * roofline: *int8_ops_per_s from back-to-back tcgen05 kind::i8 MMAs (128 x 256 x 32,
+ * one CTA per SM, operands in shared memory; ops = 2 x MACs) and *fp64_fma_per_s from
+ * eight independent FP64 FMA chains per thread (16 warps per SM).  About 20 ms of GPU
+ * time; synchronises `stream`.  No counterpart in pg_gpu (measurement support). */
+LDK_API int ldk_probe_peaks(double* int8_ops_per_s, double* fp64_fma_per_s, void* stream);
+
 /* out[r, k] = sum_b weights[r, b] * block_sums[b, k] (float64); weights int32 (R, n_blocks).
  * Block-bootstrap replicates over pre-binned per-block sums, the semantics of
  * resampling.block_bootstrap (resampling.py:201-256); also per-window totals. */

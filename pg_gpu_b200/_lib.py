@@ -75,6 +75,7 @@ EXPORTS = {
     "ldk_profile_last_kernel_ms": (ctypes.c_double, []),
     "ldk_block_combine": (ctypes.c_int, [c_vp, ctypes.c_int64, ctypes.c_int64, c_vp, ctypes.c_int64, c_vp,
                                          c_vp]),
+    "ldk_probe_peaks": (ctypes.c_int, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), c_vp]),
 }
 
 _lib = None
@@ -124,3 +125,12 @@ def ptr(t):
     if not t.is_contiguous():
         raise ValueError("expected a contiguous tensor")
     return ctypes.c_void_p(t.data_ptr())
+
+
+def probe_peaks(stream=None):
+    """Measured INT8 tensor-core ops/s (MAC = 2) and FP64 FMA/s of the current device
+    (``ldk_probe_peaks``)."""
+    require_cuda()
+    i8, f64 = ctypes.c_double(), ctypes.c_double()
+    check(load().ldk_probe_peaks(ctypes.byref(i8), ctypes.byref(f64), stream_handle(stream)))
+    return i8.value, f64.value

@@ -346,6 +346,21 @@ int ldk_profile(int enable) {
 
 double ldk_profile_last_kernel_ms(void) { return (double)g_kernel_ms; }
 
+int ldk_probe_peaks(double* int8_ops_per_s, double* fp64_fma_per_s, void* stream) {
+    if (!int8_ops_per_s || !fp64_fma_per_s) { set_error("null pointer"); return LDK_ERR_ARG; }
+    if (int rc = check_arch()) return rc;
+    *int8_ops_per_s = 0.0;
+    *fp64_fma_per_s = 0.0;
+    unsigned st = 0;
+    if (int rc = check_cuda(probe_peaks(int8_ops_per_s, fp64_fma_per_s, &st, (cudaStream_t)stream), "peak probes"))
+        return rc;
+    if (st) {
+        set_error("peak probe: %s (status 0x%x)", status_text(st), st);
+        return LDK_ERR_DEVICE;
+    }
+    return LDK_OK;
+}
+
 int ldk_block_combine(const double* block_sums, int64_t n_blocks, int64_t k, const int32_t* weights, int64_t n_rep,
                       double* out, void* stream) {
     if (n_blocks < 0 || k < 0 || n_rep < 0) { set_error("bad sizes"); return LDK_ERR_ARG; }

@@ -626,6 +626,74 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// peak probes: the two rates the fused parse's roofline is stated against
+// ---------------------------------------------------------------------------
+
+// Back-to-back kind::i8 MMAs (M = 128, N = 256, K = 32) from zero-filled shared-memory
+// tiles into one TMEM accumulator, issued by one thread per CTA.
+constexpr int kProbeN = 256;
+__device__ unsigned g_probe_status;  // LDK_DEVERR_* of the probes
+__device__ double g_probe_sink;      // keeps the FP64 chains live
+
+__global__ void __launch_bounds__(128, 1) k_probe_i8(int iters) {
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    constexpr int A_BYTES = 128 * kKChunk, B_BYTES = kProbeN * kKChunk;
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_base_s;
+    __shared__ volatile int abort_s;
+    for (int idx = threadIdx.x; idx < (A_BYTES + B_BYTES) / 16; idx += blockDim.x)
+        reinterpret_cast<uint4*>(base)[idx] = make_uint4(0u, 0u, 0u, 0u);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        abort_s = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (threadIdx.x < 32) {
+        tmem_alloc(&tmem_base_s, kProbeN);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base_s;
+    if (threadIdx.x == 0) {
+        constexpr uint32_t idesc = idesc_u8<kProbeN>();
+        const uint32_t a_addr = su32(base), b_addr = a_addr + A_BYTES;
+        for (int it = 0; it < iters; ++it)
+#pragma unroll
+            for (int ks = 0; ks < kKChunk / 32; ++ks)
+                mma_u8(tmem, sw128_desc(a_addr + ks * 32), sw128_desc(b_addr + ks * 32), idesc, (it | ks) ? 1u : 0u);
+        mma_commit(&bar);
+        mbar_wait(&bar, 0u, &abort_s, &g_probe_status);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        tc_fence_after();
+        tmem_dealloc(tmem, kProbeN);
+    }
+}
+
+// Eight independent FP64 FMA chains per thread.
+__global__ void __launch_bounds__(512) k_probe_fp64(int iters, double b, double c) {
+    double x[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = threadIdx.x * 1e-3 + k;
+    for (int it = 0; it < iters; ++it)
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+#pragma unroll
+            for (int k = 0; k < 8; ++k) x[k] = fma(x[k], b, c);
+    double t = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) t += x[k];
+    if (t == 1234.5678) g_probe_sink = t;  // never true for these inputs
+}
+
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -760,6 +828,48 @@ cudaError_t launch_parse_tc(const ldk_parse_t* d, const ldk_parse_out_t* o, cons
     }
 #undef LDK_TC_ONE
 #undef LDK_TC_CASE
+}
+
+
+// Peak probes, each timed with CUDA events on `s` after one untimed warm-up launch.
+// *status receives the probes' device status word.
+cudaError_t probe_peaks(double* int8_ops_per_s, double* fp64_fma_per_s, unsigned* status, cudaStream_t s) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t smem = 1024 + 128 * kKChunk + kProbeN * kKChunk;
+    cudaError_t e = cudaFuncSetAttribute(k_probe_i8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const unsigned zero = 0u;
+    if ((e = cudaMemcpyToSymbolAsync(g_probe_status, &zero, sizeof(unsigned), 0, cudaMemcpyHostToDevice, s)) !=
+        cudaSuccess)
+        return e;
+    cudaEvent_t e0, e1;
+    if ((e = cudaEventCreate(&e0)) != cudaSuccess) return e;
+    if ((e = cudaEventCreate(&e1)) != cudaSuccess) { cudaEventDestroy(e0); return e; }
+    float ms = 0.f;
+    const int i8_iters = 20000, f64_iters = 2000;
+    k_probe_i8<<<sms, 128, smem, s>>>(64);
+    cudaEventRecord(e0, s);
+    k_probe_i8<<<sms, 128, smem, s>>>(i8_iters);
+    cudaEventRecord(e1, s);
+    if ((e = cudaEventSynchronize(e1)) == cudaSuccess && (e = cudaEventElapsedTime(&ms, e0, e1)) == cudaSuccess)
+        *int8_ops_per_s = 2.0 * 128 * kProbeN * kKChunk * (double)i8_iters * sms / (ms * 1e-3);
+    if (e == cudaSuccess) {
+        k_probe_fp64<<<sms, 512, 0, s>>>(16, 0.999999, 1e-9);
+        cudaEventRecord(e0, s);
+        k_probe_fp64<<<sms, 512, 0, s>>>(f64_iters, 0.999999, 1e-9);
+        cudaEventRecord(e1, s);
+        if ((e = cudaEventSynchronize(e1)) == cudaSuccess && (e = cudaEventElapsedTime(&ms, e0, e1)) == cudaSuccess)
+            *fp64_fma_per_s = 64.0 * 512 * (double)f64_iters * sms / (ms * 1e-3);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaMemcpyFromSymbolAsync(status, g_probe_status, sizeof(unsigned), 0, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e;
 }
 
 }  // namespace ldk

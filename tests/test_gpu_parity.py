@@ -267,3 +267,14 @@ def test_block_combine_bootstrap():
     w = rng.integers(0, 3, size=(7, 30)).astype(np.int32)
     got = parse.block_combine(dev(bs, torch.float64), w).cpu().numpy()
     np.testing.assert_allclose(got, np.tensordot(w, bs, axes=(1, 0)), rtol=1e-13, atol=1e-13)
+
+
+def test_probe_peaks_plausible():
+    """The roofline denominators measured on this device: INT8 tensor ops/s between
+    1 and 10 POP/s (B200 nominal dense 4.5) and FP64 FMA/s between 5 and 30 T/s
+    (nominal 18.5 T FMA/s); a second call agrees with the first within 20%."""
+    i8, f64 = _lib.probe_peaks()
+    assert 1e15 < i8 < 1e16, i8
+    assert 5e12 < f64 < 3e13, f64
+    i8b, f64b = _lib.probe_peaks()
+    assert abs(i8b - i8) < 0.2 * i8 and abs(f64b - f64) < 0.2 * f64
