@@ -65,7 +65,7 @@ bool shape_of(const ldk_parse_t* d, ParseShape& sh) {
     sh.genotypes = d->genotypes;
     sh.n_stats = stats_of(d->n_pops);
     sh.n_bins = d->n_bins;
-    sh.planes = 2;
+    sh.planes = tc_planes(sh);
     int k = 0;
     sh.max_n = 0;
     for (int p = 0; p < LDK_MAX_POPS + 1; ++p) sh.kofs[p] = 0;
@@ -98,9 +98,10 @@ Layout layout_of(const ldk_parse_t* d, const ParseShape& sh) {
     off = align_up(off + (size_t)(window_count(d) + 1) * sizeof(int64_t), 256);
     if (d->method != LDK_METHOD_PLAIN_FP64) {
         int n_items = 0;
+        const int rows = tc_rows_per_block(sh);
         for (int w = 0; w < window_count(d); ++w) {
             const int64_t m = window_bound(d, w + 1) - window_bound(d, w);
-            n_items += (int)((m + 63) / 64);
+            n_items += (int)((m + rows - 1) / rows);
         }
         L.n_items = n_items;
         L.items_off = off;
@@ -139,8 +140,8 @@ int validate(const ldk_parse_t* d) {
         for (int w = 0; w < d->n_windows; ++w)
             if (d->window_offsets[w + 1] < d->window_offsets[w]) { set_error("window_offsets must not decrease"); return LDK_ERR_ARG; }
     }
-    if (d->method != LDK_METHOD_PLAIN_FP64 && d->genotypes) {
-        set_error("the tensor-core method covers the haplotype path; use LDK_METHOD_PLAIN_FP64 for genotypes");
+    if (d->method == LDK_METHOD_TC_FP32 && d->genotypes) {
+        set_error("the FP32-estimator method covers the haplotype path; use LDK_METHOD_TC for genotypes");
         return LDK_ERR_UNSUPPORTED;
     }
     return LDK_OK;
@@ -150,7 +151,7 @@ const char* status_text(unsigned s) {
     if (s & LDK_DEVERR_TIMEOUT) return "device wait timed out";
     if (s & LDK_DEVERR_BLOCK_RANGE) return "snp_block outside [0, n_blocks)";
     if (s & LDK_DEVERR_BLOCK_SPAN) return "a 64-SNP row block spans more than two bootstrap blocks";
-    if (s & LDK_DEVERR_BAD_INPUT) return "unsorted positions or coordinates, or allele codes outside {-1, 0, 1}";
+    if (s & LDK_DEVERR_BAD_INPUT) return "unsorted positions or coordinates, or allele codes outside {-1, 0, 1} (haplotypes) or {-1, 0, 1, 2} (genotypes)";
     return "device error";
 }
 
@@ -225,10 +226,12 @@ int ldk::parse_impl(const ldk_parse_t* d, const ldk_parse_out_t* out, void* work
         if (prof) cudaEventRecord(g_ev[1], s);
     } else {
         if (device_items) {
-            // row blocks of 64 SNPs in window order, listed on the device
-            if ((rc = check_cuda(launch_build_items(w, dd.n_windows, s), "row blocks"))) return rc;
+            // row blocks in window order, listed on the device
+            if ((rc = check_cuda(launch_build_items(w, dd.n_windows, tc_rows_per_block(sh), s), "row blocks")))
+                return rc;
         } else {
-            // row blocks of 64 SNPs, largest windows first (round-robin over persistent CTAs)
+            // row blocks (64 SNPs for haplotypes, 128 for genotypes), largest windows first;
+            // the kernel's CTAs claim them in this order
             std::vector<int> order(window_count(d));
             for (int k = 0; k < (int)order.size(); ++k) order[k] = k;
             std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
@@ -236,10 +239,11 @@ int ldk::parse_impl(const ldk_parse_t* d, const ldk_parse_out_t* out, void* work
             });
             std::vector<int32_t> items;
             items.reserve((size_t)L.n_items * 2);
+            const int rows = tc_rows_per_block(sh);
             for (int wi : order)
-                for (int64_t r0 = woff[wi]; r0 < woff[wi + 1]; r0 += 64) {
+                for (int64_t r0 = woff[wi]; r0 < woff[wi + 1]; r0 += rows) {
                     items.push_back((int32_t)r0);
-                    items.push_back((int32_t)std::min<int64_t>(r0 + 64, woff[wi + 1]));
+                    items.push_back((int32_t)std::min<int64_t>(r0 + rows, woff[wi + 1]));
                 }
             if (!items.empty() &&
                 (rc = check_cuda(cudaMemcpyAsync(w.items, items.data(), items.size() * sizeof(int32_t),

@@ -52,10 +52,11 @@ cudaError_t launch_prep_planes(const ldk_parse_t* d, const Scratch& w, const Par
 cudaError_t launch_parse_tc(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w,
                             const ParseShape& sh, int n_items, cudaStream_t s);
 int tc_rows_per_block(const ParseShape& sh);
+int tc_planes(const ParseShape& sh);
 cudaError_t probe_peaks(double* int8_ops_per_s, double* fp64_fma_per_s, unsigned* status, cudaStream_t s);
 size_t tc_smem_bytes(const ParseShape& sh);
 
-cudaError_t launch_build_items(const Scratch& w, int n_windows, cudaStream_t s);
+cudaError_t launch_build_items(const Scratch& w, int n_windows, int rows, cudaStream_t s);
 
 // ldk_parse with a caller-provided workspace; device_items lists the tensor-core row
 // blocks with a device kernel (window order) instead of a host-built upload.

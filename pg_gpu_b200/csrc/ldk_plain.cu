@@ -410,13 +410,13 @@ cudaError_t launch_parse_plain_t(const PlainArgs& a, int nb, cudaStream_t s) {
 }
 
 // Row blocks of 64 SNPs per window, in window order (one thread: a setup step).
-__global__ void k_build_items(const int64_t* __restrict__ win_off, int n_win, int32_t* __restrict__ items) {
+__global__ void k_build_items(const int64_t* __restrict__ win_off, int n_win, int rows, int32_t* __restrict__ items) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     int k = 0;
     for (int wi = 0; wi < n_win; ++wi)
-        for (int64_t r0 = win_off[wi]; r0 < win_off[wi + 1]; r0 += 64) {
+        for (int64_t r0 = win_off[wi]; r0 < win_off[wi + 1]; r0 += rows) {
             items[2 * k] = (int32_t)r0;
-            const int64_t r1 = r0 + 64 < win_off[wi + 1] ? r0 + 64 : win_off[wi + 1];
+            const int64_t r1 = r0 + rows < win_off[wi + 1] ? r0 + rows : win_off[wi + 1];
             items[2 * k + 1] = (int32_t)r1;
             ++k;
         }
@@ -525,8 +525,8 @@ cudaError_t launch_parse_plain(const ldk_parse_t* d, const ldk_parse_out_t* o, c
 #undef LDK_PLAIN_CASE
 }
 
-cudaError_t launch_build_items(const Scratch& w, int n_windows, cudaStream_t s) {
-    k_build_items<<<1, 1, 0, s>>>(w.win_off, n_windows, w.items);
+cudaError_t launch_build_items(const Scratch& w, int n_windows, int rows, cudaStream_t s) {
+    k_build_items<<<1, 1, 0, s>>>(w.win_off, n_windows, rows, w.items);
     return cudaGetLastError();
 }
 

@@ -40,27 +40,42 @@ namespace ldk {
 
 namespace {
 
-constexpr int kRows = 64;               // SNPs per row block (M = 128 = 64 x {h, v})
 constexpr int kKChunk = 128;            // K bytes per TMA box / swizzle row
 constexpr int kEpi = 4;                 // epilogue warps, one per TMEM lane quarter
-constexpr int kSlots = 2;               // bootstrap blocks staged per row block
 constexpr int kRing = 2;                // claimed row blocks in flight between the roles
 constexpr int kTmemCols = 512;
 constexpr uint64_t kTimeoutNs = 5000000000ull;  // 5 s per wait
 constexpr size_t kMinSmem = 116 * 1024;
 constexpr size_t kMaxSmem = 227 * 1024;
 
-template <int P>
+// Tile geometry.  Haplotype path: a row block of 64 SNPs x {h, v} = 128 MMA rows against
+// NJ partners x {h, v} (N = 2 NJ), one MMA per K step and population.  Genotype path: a row
+// block of 128 SNPs; indicator planes {g == 1, g == 2, valid}; per K step and population
+// three MMAs, plane x of the row block against all three planes of NJ = 16 partners
+// (N = 3 NJ = 48) into region x, so TMEM lane r holds all nine Gram products of SNP r.
+// Tile geometry.  Haplotype path: a row block of 64 SNPs x {h, v} = 128 MMA rows against
+// NJ partners x {h, v} (N = 2 NJ), one MMA per K step and population.  Genotype path: a row
+// block of 128 SNPs; four stored planes per SNP {g == 1, g == 2, valid, 0}; per K step and
+// population three MMAs, plane x (< 3) of the row block against all four planes of NJ
+// partners (N = 4 NJ) into region x, so TMEM lane r holds all nine Gram products of SNP r
+// (and a zero column per partner, which keeps every partner's columns 4-aligned).
+template <int P, bool GENO = false>
 struct Cfg {
-    static constexpr int NJ = (P == 1) ? 128 : (P == 2) ? 64 : 32;  // partner SNPs per tile
-    static constexpr int N = 2 * NJ;                                 // MMA N
-    static constexpr int COLS = P * N;                               // TMEM columns per buffer
-    static constexpr int STAGES = (P == 1) ? 2 : (P == 2) ? 3 : 4;
-    static constexpr int A_BYTES = 2 * kRows * kKChunk;
+    static constexpr int ROWS = GENO ? 128 : 64;                      // SNPs per row block
+    static constexpr int PLANES = GENO ? 4 : 2;                        // stored planes per SNP
+    static constexpr int NJ = GENO ? (P == 1 ? 16 : 8) : (P == 1) ? 128 : (P == 2) ? 64 : 32;  // partners per tile
+    static constexpr int N = PLANES * NJ;                              // MMA N
+    static constexpr int REGIONS = GENO ? 3 : 1;                       // MMAs per K step and population
+    static constexpr int COLS = P * REGIONS * N;                       // TMEM columns per buffer
+    static constexpr int NBUF = 2 * COLS <= kTmemCols ? 2 : 1;         // accumulator buffers
+    static constexpr int STAGES = GENO ? 3 : (P == 1) ? 2 : (P == 2) ? 3 : 4;
+    static constexpr int A_BOX = 128 * kKChunk;                        // one 128-row A box
+    static constexpr int A_BYTES = REGIONS * A_BOX;
     static constexpr int B_BYTES = N * kKChunk;
     static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
     static constexpr int NS = HapNStats<P>::value;
-    static_assert(2 * COLS <= kTmemCols, "TMEM budget");
+    static constexpr int SLOTS = GENO ? 4 : 2;                         // bootstrap blocks staged per row block
+    static_assert(NBUF * COLS <= kTmemCols, "TMEM budget");
     static_assert(N % 16 == 0 && N <= 256, "MMA N");
 };
 
@@ -215,7 +230,8 @@ LDK_DEV void spin_ns(uint64_t ns) {
 }
 
 // ---------------------------------------------------------------------------
-// indicator planes: planes[v][0][k] = [x == 1], planes[v][1][k] = [x in {0, 1}]
+// indicator planes.  Haplotypes: planes[v][0][k] = [x == 1], planes[v][1][k] = [x in {0, 1}].
+// Genotypes: planes[v][0..3][k] = [x == 1], [x == 2], [x in {0, 1, 2}], 0.
 // ---------------------------------------------------------------------------
 
 struct PrepArgs {
@@ -227,16 +243,24 @@ struct PrepArgs {
     int kofs[LDK_MAX_POPS + 1];
     int P;
     int ktot;
-    uint8_t* planes;
+    int genotypes;
+    int planes;
+    uint8_t* planes_out;
     unsigned* status;
 };
 
 constexpr int kPrepV = 64, kPrepK = 128;
 
+LDK_DEV uint32_t plane_bit(int8_t x, int plane, int genotypes) {
+    if (genotypes) return plane == 0 ? (x == 1) : plane == 1 ? (x == 2) : plane == 2 ? (x >= 0 && x <= 2) : 0u;
+    return plane == 0 ? (x == 1) : (x == 0 || x == 1);
+}
+
 __global__ void __launch_bounds__(256) k_prep_planes(PrepArgs a) {
     __shared__ int8_t tile[kPrepK][kPrepV + 4];
     const int64_t v0 = (int64_t)blockIdx.x * kPrepV;
     const int k0 = blockIdx.y * kPrepK;
+    const int xmax = a.genotypes ? 2 : 1;
     // gather: tile[k][v] = X[row(k), v0 + v] (coalesced along v); 127 marks padding
     for (int idx = threadIdx.x; idx < kPrepK * kPrepV; idx += blockDim.x) {
         const int kk = idx / kPrepV, vv = idx % kPrepV;
@@ -251,27 +275,23 @@ __global__ void __launch_bounds__(256) k_prep_planes(PrepArgs a) {
             if (local >= 0 && local < np && k < a.kofs[a.P]) {
                 const int row = a.pop_rows[a.pop_off[p] + local];
                 x = a.X[(int64_t)row * a.ld + v];
-                if (x < -1 || x > 1) atomicOr(a.status, LDK_DEVERR_BAD_INPUT);
+                if (x < -1 || x > xmax) atomicOr(a.status, LDK_DEVERR_BAD_INPUT);
             }
         }
         tile[kk][vv] = x;
     }
     __syncthreads();
     // scatter: 4 bytes of one plane per thread, coalesced along k
-    for (int idx = threadIdx.x; idx < kPrepV * 2 * (kPrepK / 4); idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < kPrepV * a.planes * (kPrepK / 4); idx += blockDim.x) {
         const int kq = idx % (kPrepK / 4);
-        const int plane = (idx / (kPrepK / 4)) % 2;
-        const int vv = idx / (2 * (kPrepK / 4));
+        const int plane = (idx / (kPrepK / 4)) % a.planes;
+        const int vv = idx / (a.planes * (kPrepK / 4));
         const int64_t v = v0 + vv;
         if (v >= a.n_var) continue;
         uint32_t w = 0;
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const int8_t x = tile[4 * kq + b][vv];
-            const uint32_t bit = plane == 0 ? (x == 1) : (x == 0 || x == 1);
-            w |= bit << (8 * b);
-        }
-        *reinterpret_cast<uint32_t*>(a.planes + (v * 2 + plane) * (int64_t)a.ktot + k0 + 4 * kq) = w;
+        for (int b = 0; b < 4; ++b) w |= plane_bit(tile[4 * kq + b][vv], plane, a.genotypes) << (8 * b);
+        *reinterpret_cast<uint32_t*>(a.planes_out + (v * a.planes + plane) * (int64_t)a.ktot + k0 + 4 * kq) = w;
     }
 }
 
@@ -298,21 +318,22 @@ struct TcArgs {
     unsigned* status;
 };
 
-template <int P, typename T, bool PRIV>
+template <int P, typename T, bool PRIV, bool GENO>
 __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
     k_parse_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcArgs a) {
-    using C = Cfg<P>;
+    using C = Cfg<P, GENO>;
     constexpr int NS = C::NS;
+    constexpr int SLOTS = C::SLOTS;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int nb = a.edges.n_bins;
     unsigned char* stages = base;
     constexpr int NCOPY = PRIV ? kEpi : 1;  // staging copies: one per epilogue warp, or shared
-    double* sacc = reinterpret_cast<double*>(base + C::STAGES * C::STAGE_BYTES);  // [NCOPY][kSlots][nb][NS+1]
-    unsigned* scnt = reinterpret_cast<unsigned*>(sacc + NCOPY * kSlots * nb * (NS + 1));  // [NCOPY][kSlots][nb][2]
-    double4* rtab = reinterpret_cast<double4*>(scnt + ((NCOPY * kSlots * nb * 2 + 7) & ~7));  // [max_n + 1]
+    double* sacc = reinterpret_cast<double*>(base + C::STAGES * C::STAGE_BYTES);  // [NCOPY][SLOTS][nb][NS+1]
+    unsigned* scnt = reinterpret_cast<unsigned*>(sacc + NCOPY * SLOTS * nb * (NS + 1));  // [NCOPY][SLOTS][nb][2]
+    double4* rtab = reinterpret_cast<double4*>(scnt + ((NCOPY * SLOTS * nb * 2 + 7) & ~7));  // [max_n + 1]
 
-    __shared__ __align__(8) uint64_t full_bar[C::STAGES], empty_bar[C::STAGES], tfull[2], tempty[2];
+    __shared__ __align__(8) uint64_t full_bar[C::STAGES], empty_bar[C::STAGES], tfull[C::NBUF], tempty[C::NBUF];
     __shared__ __align__(8) uint64_t ifull[kRing], iempty[kRing];
     __shared__ volatile int ring[kRing];
     __shared__ uint32_t tmem_base_s;
@@ -325,7 +346,7 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
             mbar_init(&full_bar[s], 1);
             mbar_init(&empty_bar[s], 1);
         }
-        for (int b = 0; b < 2; ++b) {
+        for (int b = 0; b < C::NBUF; ++b) {
             mbar_init(&tfull[b], 1);
             mbar_init(&tempty[b], kEpi);
         }
@@ -337,9 +358,10 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int b = threadIdx.x; b <= nb; b += blockDim.x) sedges[b] = a.edges.e[b];
-    for (int idx = threadIdx.x; idx < NCOPY * kSlots * nb * (NS + 1); idx += blockDim.x) sacc[idx] = 0.0;
-    for (int idx = threadIdx.x; idx < NCOPY * kSlots * nb * 2; idx += blockDim.x) scnt[idx] = 0u;
-    for (int idx = threadIdx.x; idx <= a.max_n; idx += blockDim.x) rtab[idx] = recip_entry(idx);
+    for (int idx = threadIdx.x; idx < NCOPY * SLOTS * nb * (NS + 1); idx += blockDim.x) sacc[idx] = 0.0;
+    for (int idx = threadIdx.x; idx < NCOPY * SLOTS * nb * 2; idx += blockDim.x) scnt[idx] = 0u;
+    if constexpr (!GENO)
+        for (int idx = threadIdx.x; idx <= a.max_n; idx += blockDim.x) rtab[idx] = recip_entry(idx);
     if (warp == 1) {
         tmem_alloc(&tmem_base_s, kTmemCols);
         tmem_relinquish();
@@ -373,7 +395,9 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
                         if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_s, a.status)) { ok = false; break; }
                         unsigned char* dst = stages + s * C::STAGE_BYTES;
                         mbar_expect_tx(&full_bar[s], C::STAGE_BYTES);
-                        tma_load_3d(dst, &tmA, &full_bar[s], c * kKChunk, 0, row0);
+#pragma unroll
+                        for (int x = 0; x < C::REGIONS; ++x)
+                            tma_load_3d(dst + x * C::A_BOX, &tmA, &full_bar[s], c * kKChunk, x, row0);
                         tma_load_3d(dst + C::A_BYTES, &tmB, &full_bar[s], c * kKChunk, 0, j0);
                     }
                 }
@@ -397,7 +421,7 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
                 const int jend = a.jmax[row1 - 1];
                 const int n_jt = jend > row0 + 1 ? (jend - row0 + C::NJ - 1) / C::NJ : 0;
                 for (int t = 0; t < n_jt && ok; ++t, ++tcount) {
-                    const uint32_t buf = tcount & 1u, tph = (tcount >> 1) & 1u;
+                    const uint32_t buf = tcount % C::NBUF, tph = (tcount / C::NBUF) & 1u;
                     if (!mbar_wait(&tempty[buf], tph ^ 1u, &abort_s, a.status)) { ok = false; break; }
                     tc_fence_after();
                     for (int c = 0; c < a.nkc; ++c, ++it) {
@@ -414,8 +438,12 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
 #pragma unroll
                             for (int q = 1; q < P; ++q) p += (kbyte >= a.kofs[q]) ? 1 : 0;
                             const uint32_t first = (kbyte == a.kofs[p]) ? 1u : 0u;
-                            const uint32_t d = tmem + buf * C::COLS + p * C::N;
-                            mma_u8(d, sw128_desc(a_addr + ks * 32), sw128_desc(b_addr + ks * 32), idesc, first ^ 1u);
+#pragma unroll
+                            for (int x = 0; x < C::REGIONS; ++x) {
+                                const uint32_t d = tmem + buf * C::COLS + (p * C::REGIONS + x) * C::N;
+                                mma_u8(d, sw128_desc(a_addr + x * C::A_BOX + ks * 32), sw128_desc(b_addr + ks * 32),
+                                       idesc, first ^ 1u);
+                            }
                         }
                         mma_commit(&empty_bar[s]);
                     }
@@ -431,11 +459,15 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
         // ------------------------------------------------------------- epilogue
         const int e = warp - 4;
         const int L = (warp & 3) * 32 + lane;
-        const int r = L >> 1, role = L & 1;
+        // haplotype rows: lanes 2r, 2r+1 share SNP r and split its partners by parity;
+        // genotype rows: lane L is SNP L and takes every partner
+        const int r = GENO ? L : L >> 1, role = GENO ? 0 : L & 1;
         const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
-        const int stage_n = kSlots * nb * (NS + 1);
+        const int stage_n = SLOTS * nb * (NS + 1);
         double* my_sacc = sacc + (PRIV ? e * stage_n : 0);
-        unsigned* my_scnt = scnt + (PRIV ? e * kSlots * nb * 2 : 0);
+        unsigned* my_scnt = scnt + (PRIV ? e * SLOTS * nb * 2 : 0);
+        constexpr int STEPS = GENO ? C::NJ : C::NJ / 2;   // TMEM reads per tile
+        constexpr int CREGS = (C::NJ + 31) / 32;          // partner coordinates per lane
         uint32_t tcount = 0;
         for (uint32_t k = 0;; ++k) {
             const int sl = k % kRing;
@@ -460,7 +492,7 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
             int slot = 0;
             if (row_ok && a.snp_block) {
                 slot = a.snp_block[i] - blk0;
-                if (slot < 0 || slot >= kSlots) {
+                if (slot < 0 || slot >= SLOTS) {
                     atomicOr(a.status, LDK_DEVERR_BLOCK_SPAN);
                     row_ok = false;
                 }
@@ -506,51 +538,41 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
             };
             bool ok = true;
             for (int t = 0; t < n_jt; ++t, ++tcount) {
-                const uint32_t buf = tcount & 1u, tph = (tcount >> 1) & 1u;
+                const uint32_t buf = tcount % C::NBUF, tph = (tcount / C::NBUF) & 1u;
                 const int j0 = row0 + t * C::NJ;
                 // partner coordinates of this tile, one per lane and register
-                double creg[C::NJ / 32];
+                double creg[CREGS];
 #pragma unroll
-                for (int k = 0; k < C::NJ / 32; ++k) {
-                    const int j = j0 + 32 * k + lane;
-                    creg[k] = j < jend ? a.coord[j] : 0.0;
+                for (int kk = 0; kk < CREGS; ++kk) {
+                    const int j = j0 + 32 * kk + lane;
+                    creg[kk] = (32 * kk + lane < C::NJ && j < jend) ? a.coord[j] : 0.0;
                 }
                 if (!mbar_wait(&tfull[buf], tph, &abort_s, a.status)) { ok = false; break; }
                 tc_fence_after();
-                // Two partners per step: 4 TMEM columns per population, indexed with
-                // constants only so the counts stay in registers.
+                // One TMEM read per step, indexed with constants only so the counts stay in
+                // registers.  Haplotypes: two partners per step, 4 columns per population.
+                // Genotypes: one partner per step, 4 columns per region and population.
 #pragma unroll 1
-                for (int q = 0; q < C::NJ / 2; ++q) {
-                    uint32_t v[P][4];
-                    const uint32_t col = buf * C::COLS + q * 4;
+                for (int q = 0; q < STEPS; ++q) {
+                    uint32_t v[P][C::REGIONS][4];
 #pragma unroll
-                    for (int p = 0; p < P; ++p) tmem_ld4(tmem + lane_base + col + p * C::N, v[p]);
-                    const int jj = 2 * q + role;
+                    for (int p = 0; p < P; ++p)
+#pragma unroll
+                        for (int x = 0; x < C::REGIONS; ++x)
+                            tmem_ld4(tmem + lane_base + buf * C::COLS + (p * C::REGIONS + x) * C::N + q * 4,
+                                     v[p][x]);
+                    const int jj = GENO ? q : 2 * q + role;
                     double csrc = creg[0];
 #pragma unroll
-                    for (int k = 1; k < C::NJ / 32; ++k)
-                        if ((q >> 4) == k) csrc = creg[k];
+                    for (int kk = 1; kk < CREGS; ++kk)
+                        if ((jj >> 5) == kk) csrc = creg[kk];
                     const double cj = __shfl_sync(0xffffffffu, csrc, jj & 31);
-                    tmem_wait4<P>(v);
-                    if (q == C::NJ / 2 - 1) {
+#pragma unroll
+                    for (int p = 0; p < P; ++p) tmem_wait4<C::REGIONS>(v[p]);
+                    if (q == STEPS - 1) {
                         tc_fence_before();
                         __syncwarp();
                         if (lane == 0) mbar_arrive(&tempty[buf]);
-                    }
-                    HapFeat<T> f[P];
-                    int nval[P];
-#pragma unroll
-                    for (int p = 0; p < P; ++p) {
-                        // lane 2r: (hh, hv) of partners 2q, 2q+1; lane 2r+1: (vh, vv)
-                        const uint32_t sx = role ? v[p][0] : v[p][2];
-                        const uint32_t sy = role ? v[p][1] : v[p][3];
-                        const uint32_t rx = __shfl_xor_sync(0xffffffffu, sx, 1);
-                        const uint32_t ry = __shfl_xor_sync(0xffffffffu, sy, 1);
-                        int hh, hv, vh, vv;
-                        if (role == 0) { hh = (int)v[p][0]; hv = (int)v[p][1]; vh = (int)rx; vv = (int)ry; }
-                        else { vh = (int)v[p][2]; vv = (int)v[p][3]; hh = (int)rx; hv = (int)ry; }
-                        hap_set_counts(f[p], T(hh), T(hv - hh), T(vh - hh), T(vv - hv - vh + hh));
-                        nval[p] = vv;
                     }
                     const int j = j0 + jj;
                     const bool valid = row_ok && j > i && j < my_jmax;
@@ -565,16 +587,63 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
                         for (int s = 0; s <= NS; ++s) acc[s] = T(0);
                         np = nr2 = 0;
                     }
-                    if (valid && cur >= 0 && cur < nb) {
+                    if constexpr (!GENO) {
+                        HapFeat<T> f[P];
+                        int nval[P];
 #pragma unroll
                         for (int p = 0; p < P; ++p) {
-                            hap_features<T, P>(f[p]);
-                            hap_reciprocals_from(f[p], rtab[nval[p]]);
+                            // lane 2r: (hh, hv) of partners 2q, 2q+1; lane 2r+1: (vh, vv)
+                            const uint32_t* w = v[p][0];
+                            const uint32_t sx = role ? w[0] : w[2];
+                            const uint32_t sy = role ? w[1] : w[3];
+                            const uint32_t rx = __shfl_xor_sync(0xffffffffu, sx, 1);
+                            const uint32_t ry = __shfl_xor_sync(0xffffffffu, sy, 1);
+                            int hh, hv, vh, vv;
+                            if (role == 0) { hh = (int)w[0]; hv = (int)w[1]; vh = (int)rx; vv = (int)ry; }
+                            else { vh = (int)w[2]; vv = (int)w[3]; hh = (int)rx; hv = (int)ry; }
+                            hap_set_counts(f[p], T(hh), T(hv - hh), T(vh - hh), T(vv - hv - vh + hh));
+                            nval[p] = vv;
                         }
-                        hap_fused<T, P, 0>(f, acc);
-                        T r2;
-                        if (hap_r2(f[0], r2)) { acc[NS] += r2; ++nr2; }
-                        ++np;
+                        if (valid && cur >= 0 && cur < nb) {
+#pragma unroll
+                            for (int p = 0; p < P; ++p) {
+                                hap_features<T, P>(f[p]);
+                                hap_reciprocals_from(f[p], rtab[nval[p]]);
+                            }
+                            hap_fused<T, P, 0>(f, acc);
+                            T r2;
+                            if (hap_r2(f[0], r2)) { acc[NS] += r2; ++nr2; }
+                            ++np;
+                        }
+                    } else {
+                        if (valid && cur >= 0 && cur < nb) {
+                            // Gram products G[x][y] = plane x of SNP i . plane y of SNP j
+                            // (0: g == 1, 1: g == 2, 2: valid); cells in the order of pg_gpu's
+                            // counting kernel, column g_i * 3 + g_j (ld_pipeline.py:183-263)
+                            GenoFeat<T> f[P];
+                            T c0[9];
+#pragma unroll
+                            for (int p = 0; p < P; ++p) {
+                                const uint32_t (&G)[3][4] = v[p];
+                                const int n11 = (int)G[0][0], n12 = (int)G[0][1], n21 = (int)G[1][0], n22 = (int)G[1][1];
+                                const int n10 = (int)G[0][2] - n11 - n12, n20 = (int)G[1][2] - n21 - n22;
+                                const int n01 = (int)G[2][0] - n11 - n21, n02 = (int)G[2][1] - n12 - n22;
+                                const int nv = (int)G[2][2];
+                                const int n00 = nv - n01 - n02 - n10 - n11 - n12 - n20 - n21 - n22;
+                                const T cd[9] = {T(n00), T(n01), T(n02), T(n10), T(n11), T(n12), T(n20), T(n21), T(n22)};
+                                if (p == 0) {
+#pragma unroll
+                                    for (int m = 0; m < 9; ++m) c0[m] = cd[m];
+                                }
+                                geno_set_counts(f[p], cd);
+                                f[p].n = T(nv);
+                                geno_features<T, P>(f[p]);
+                            }
+                            geno_stats<T, P>(f, acc);
+                            T r2;
+                            if (geno_dosage_r2(c0, r2)) { acc[NS] += r2; ++nr2; }
+                            ++np;
+                        }
                     }
                 }
             }
@@ -599,11 +668,11 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
                     else atomicAdd(&a.r2_sums[(int64_t)blk * nb + bb], val);
                 }
             }
-            for (int idx = et; idx < kSlots * nb; idx += 32 * kEpi) {
+            for (int idx = et; idx < SLOTS * nb; idx += 32 * kEpi) {
                 unsigned long long c0 = 0, c1 = 0;
 #pragma unroll
                 for (int w = 0; w < (PRIV ? kEpi : 1); ++w) {
-                    unsigned* sc = scnt + w * kSlots * nb * 2;
+                    unsigned* sc = scnt + w * SLOTS * nb * 2;
                     c0 += sc[2 * idx];
                     c1 += sc[2 * idx + 1];
                     sc[2 * idx] = 0u;
@@ -625,7 +694,6 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
         tmem_dealloc(tmem, kTmemCols);
     }
 }
-
 
 // ---------------------------------------------------------------------------
 // peak probes: the two rates the fused parse's roofline is stated against
@@ -711,12 +779,14 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-bool make_map(CUtensorMap* m, const uint8_t* planes, int64_t n_var, int ktot, int rows_box) {
+// planes[snp][plane][k]: boxes of 128 k x plane_box planes x rows_box SNPs
+bool make_map(CUtensorMap* m, const uint8_t* planes, int64_t n_var, int ktot, int n_planes, int plane_box,
+              int rows_box) {
     auto fn = encode_fn();
     if (!fn) return false;
-    cuuint64_t dims[3] = {(cuuint64_t)ktot, 2, (cuuint64_t)n_var};
-    cuuint64_t strides[2] = {(cuuint64_t)ktot, (cuuint64_t)ktot * 2};
-    cuuint32_t box[3] = {(cuuint32_t)kKChunk, 2, (cuuint32_t)rows_box};
+    cuuint64_t dims[3] = {(cuuint64_t)ktot, (cuuint64_t)n_planes, (cuuint64_t)n_var};
+    cuuint64_t strides[2] = {(cuuint64_t)ktot, (cuuint64_t)ktot * n_planes};
+    cuuint32_t box[3] = {(cuuint32_t)kKChunk, (cuuint32_t)plane_box, (cuuint32_t)rows_box};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<uint8_t*>(planes), dims, strides, box, estr,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -724,28 +794,34 @@ bool make_map(CUtensorMap* m, const uint8_t* planes, int64_t n_var, int ktot, in
     return r == CUDA_SUCCESS;
 }
 
-template <int P>
+template <int P, bool GENO>
 size_t smem_bytes_t(int nb, int max_n, int ncopy) {
-    using C = Cfg<P>;
-    return 1024 + (size_t)C::STAGES * C::STAGE_BYTES + (size_t)ncopy * kSlots * nb * (C::NS + 1) * sizeof(double) +
-           (size_t)((ncopy * kSlots * nb * 2 + 7) & ~7) * sizeof(unsigned) + (size_t)(max_n + 1) * sizeof(double4) + 32;
+    using C = Cfg<P, GENO>;
+    return 1024 + (size_t)C::STAGES * C::STAGE_BYTES + (size_t)ncopy * C::SLOTS * nb * (C::NS + 1) * sizeof(double) +
+           (size_t)((ncopy * C::SLOTS * nb * 2 + 7) & ~7) * sizeof(unsigned) + (size_t)(max_n + 1) * sizeof(double4) + 32;
 }
 
 // Per-warp staging copies when they fit next to the pipeline stages.
-template <int P>
-bool private_staging(int nb, int max_n) { return smem_bytes_t<P>(nb, max_n, kEpi) <= kMaxSmem; }
+template <int P, bool GENO>
+bool private_staging(int nb, int max_n) { return smem_bytes_t<P, GENO>(nb, max_n, kEpi) <= kMaxSmem; }
+
+template <bool GENO>
+size_t tc_smem_bytes_g(const ParseShape& sh) {
+    switch (sh.P) {
+        case 1: return smem_bytes_t<1, GENO>(sh.n_bins, sh.max_n, 1);
+        case 2: return smem_bytes_t<2, GENO>(sh.n_bins, sh.max_n, 1);
+        case 3: return smem_bytes_t<3, GENO>(sh.n_bins, sh.max_n, 1);
+        default: return smem_bytes_t<4, GENO>(sh.n_bins, sh.max_n, 1);
+    }
+}
 
 }  // namespace
 
-int tc_rows_per_block(const ParseShape&) { return kRows; }
+int tc_rows_per_block(const ParseShape& sh) { return sh.genotypes ? Cfg<1, true>::ROWS : Cfg<1, false>::ROWS; }
+int tc_planes(const ParseShape& sh) { return sh.genotypes ? Cfg<1, true>::PLANES : Cfg<1, false>::PLANES; }
 
 size_t tc_smem_bytes(const ParseShape& sh) {
-    switch (sh.P) {
-        case 1: return smem_bytes_t<1>(sh.n_bins, sh.max_n, 1);
-        case 2: return smem_bytes_t<2>(sh.n_bins, sh.max_n, 1);
-        case 3: return smem_bytes_t<3>(sh.n_bins, sh.max_n, 1);
-        default: return smem_bytes_t<4>(sh.n_bins, sh.max_n, 1);
-    }
+    return sh.genotypes ? tc_smem_bytes_g<true>(sh) : tc_smem_bytes_g<false>(sh);
 }
 
 cudaError_t launch_prep_planes(const ldk_parse_t* d, const Scratch& w, const ParseShape& sh, cudaStream_t s) {
@@ -761,19 +837,24 @@ cudaError_t launch_prep_planes(const ldk_parse_t* d, const Scratch& w, const Par
     }
     a.P = sh.P;
     a.ktot = sh.ktot;
-    a.planes = w.hv;
+    a.genotypes = sh.genotypes;
+    a.planes = sh.planes;
+    a.planes_out = w.hv;
     a.status = w.status;
     dim3 grid((unsigned)((d->n_var + kPrepV - 1) / kPrepV), (unsigned)(sh.ktot / kPrepK));
     k_prep_planes<<<grid, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 
-template <int P, typename T, bool PRIV>
+template <int P, typename T, bool PRIV, bool GENO>
 static cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w,
                                      const ParseShape& sh, int n_items, cudaStream_t s) {
-    using C = Cfg<P>;
+    using C = Cfg<P, GENO>;
+    // A: the row block (haplotypes: both planes of 64 SNPs; genotypes: one plane of 128
+    // SNPs per box); B: every plane of NJ partners
     CUtensorMap mA, mB;
-    if (!make_map(&mA, w.hv, d->n_var, sh.ktot, kRows) || !make_map(&mB, w.hv, d->n_var, sh.ktot, C::NJ))
+    if (!make_map(&mA, w.hv, d->n_var, sh.ktot, C::PLANES, GENO ? 1 : C::PLANES, C::ROWS) ||
+        !make_map(&mB, w.hv, d->n_var, sh.ktot, C::PLANES, C::PLANES, C::NJ))
         return cudaErrorInvalidValue;
     TcArgs a;
     a.coord = d->coord ? d->coord : d->pos;
@@ -795,30 +876,32 @@ static cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t
     a.status = w.status;
     // at least half of an SM's shared memory, so that one CTA (holding all 512 TMEM
     // columns) runs per SM
-    size_t smem = smem_bytes_t<P>(d->n_bins, sh.max_n, PRIV ? kEpi : 1);
+    size_t smem = smem_bytes_t<P, GENO>(d->n_bins, sh.max_n, PRIV ? kEpi : 1);
     if (smem < kMinSmem) smem = kMinSmem;
     if (smem > kMaxSmem) return cudaErrorInvalidConfiguration;
-    cudaError_t e = cudaFuncSetAttribute(k_parse_tc<P, T, PRIV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_parse_tc<P, T, PRIV, GENO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (n_items == 0) return cudaSuccess;
     const int grid = n_items < sms ? n_items : sms;
-    k_parse_tc<P, T, PRIV><<<grid, 128 + 32 * kEpi, smem, s>>>(mA, mB, a);
+    k_parse_tc<P, T, PRIV, GENO><<<grid, 128 + 32 * kEpi, smem, s>>>(mA, mB, a);
     return cudaGetLastError();
 }
 
 cudaError_t launch_parse_tc(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w,
                             const ParseShape& sh, int n_items, cudaStream_t s) {
     const bool f32 = d->method == LDK_METHOD_TC_FP32;
-#define LDK_TC_ONE(PP, TT)                                                                          \
-    return private_staging<PP>(sh.n_bins, sh.max_n) ? launch_parse_tc_p<PP, TT, true>(d, o, w, sh, n_items, s) \
-                                                    : launch_parse_tc_p<PP, TT, false>(d, o, w, sh, n_items, s);
-#define LDK_TC_CASE(PP)                                                                             \
-    case PP:                                                                                        \
-        if (f32) { LDK_TC_ONE(PP, float) }                                                          \
-        LDK_TC_ONE(PP, double)
+#define LDK_TC_ONE(PP, TT, GG)                                                                              \
+    return private_staging<PP, GG>(sh.n_bins, sh.max_n) ? launch_parse_tc_p<PP, TT, true, GG>(d, o, w, sh, n_items, s) \
+                                                        : launch_parse_tc_p<PP, TT, false, GG>(d, o, w, sh, n_items, s);
+#define LDK_TC_CASE(PP)                                                                                     \
+    case PP:                                                                                                \
+        if (sh.genotypes) { LDK_TC_ONE(PP, double, true) }                                                  \
+        if (f32) { LDK_TC_ONE(PP, float, false) }                                                           \
+        LDK_TC_ONE(PP, double, false)
     switch (sh.P) {
         LDK_TC_CASE(1)
         LDK_TC_CASE(2)

@@ -207,7 +207,7 @@ def test_parse_plain_matches_oracle(workloads, oracle_results, k):
     check_parse(run_parse(workloads[k], "plain"), oracle_results[k], PLAIN_RTOL)
 
 
-@pytest.mark.parametrize("k", [1, 2, 4, 5])
+@pytest.mark.parametrize("k", [1, 2, 3, 4, 5])
 def test_parse_tc_matches_oracle(workloads, oracle_results, k):
     check_parse(run_parse(workloads[k], "tc"), oracle_results[k], TC_RTOL)
 
@@ -246,6 +246,56 @@ def test_parse_edge_cases():
         want = O.bin_sums(hap, pos, rows, [0.0, 100.0, 1000.0], window_offsets=wo)
         np.testing.assert_array_equal(r["pairs"], want["pairs"])
         assert rel_err(r["sums"], want["sums"], 1e-300) < (PLAIN_RTOL if method == "plain" else TC_RTOL)
+
+
+def _genotypes(rng, n_ind, n_var, missing):
+    """Genotypes as sums of two correlated haplotypes (a few founders), with missing calls."""
+    founders = (rng.random((6, n_var)) < rng.uniform(0.05, 0.6, n_var)).astype(np.int8)
+    h = founders[rng.integers(0, 6, size=(2 * n_ind,))]
+    flip = rng.random(h.shape) < 0.05
+    h = np.where(flip, 1 - h, h).astype(np.int8)
+    g = (h[0::2] + h[1::2]).astype(np.int8)
+    g[rng.random(g.shape) < missing] = -1
+    return g
+
+
+@pytest.mark.parametrize("P", [1, 2, 3, 4])
+def test_parse_tc_genotypes_windows_blocks(P):
+    """Genotype path on tensor cores: 128-SNP row blocks, several populations of unequal
+    size, windows of 0, 1, 3 and many SNPs, bootstrap blocks up to four per row block."""
+    rng = np.random.default_rng(100 + P)
+    sizes = [17, 40, 9, 33][:P]
+    n_var = 700
+    g = _genotypes(rng, sum(sizes), n_var, 0.03)
+    pos = np.cumsum(rng.integers(1, 40, size=n_var)).astype(np.float64)
+    offs = np.cumsum([0] + sizes)
+    rows = [np.arange(offs[p], offs[p + 1]) for p in range(P)]
+    wo = np.array([0, 0, 1, 4, 300, n_var])
+    blocks = np.minimum(pos // 1500, 1e9).astype(np.int32)
+    nblk = int(blocks.max()) + 1
+    edges = np.array([0.0, 50.0, 200.0, 800.0, 3000.0])
+    want = O.bin_sums(g, pos, rows, edges, genotypes=True, max_dist=2500.0, window_offsets=wo,
+                      snp_block=blocks, n_blocks=nblk)
+    assert want["pairs"].sum() > 0
+    for method, tol in (("plain", PLAIN_RTOL), ("tc", TC_RTOL)):
+        r = parse.ld_parse(g, pos, rows, edges, genotypes=True, method=method, max_dist=2500.0,
+                           window_offsets=wo, snp_block=blocks, n_blocks=nblk).numpy()
+        check_parse(r, want, tol)
+
+
+def test_parse_tc_genotype_edge_cases():
+    rng = np.random.default_rng(7)
+    g = _genotypes(rng, 25, 300, 0.0)
+    g[:, 5] = 0          # monomorphic site: r^2 undefined, statistics still counted
+    g[:, 6] = -1         # a site missing everywhere: n_valid 0
+    pos = np.arange(300, dtype=np.float64) * 7.0
+    rows = [np.arange(25)]
+    for edges, md in (([0.0, 5.0], 0.0), ([14.0, 70.0, 700.0], None), ([0.0, 10.0, 2100.0], None)):
+        want = O.bin_sums(g, pos, rows, edges, genotypes=True, max_dist=md)
+        r = parse.ld_parse(g, pos, rows, edges, genotypes=True, method="tc", max_dist=md).numpy()
+        np.testing.assert_array_equal(r["pairs"], want["pairs"])
+        np.testing.assert_array_equal(r["r2_counts"], want["r2_count"])
+        assert rel_err(r["sums"], want["sums"], 1e-300) < TC_RTOL
 
 
 def test_parse_reports_errors():
