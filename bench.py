@@ -116,11 +116,11 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 
 def _cpu_task(args):
-    data, pos, pop_rows, edges, max_dist, n_pairs = args
+    data, pos, pop_rows, edges, max_dist, n_pairs, genotypes = args
     os.environ.setdefault("OMP_NUM_THREADS", "1")
     from oracle import ld_oracle as O
     t0 = time.perf_counter()
-    r = O.bin_sums(data, pos, pop_rows, edges, max_dist=max_dist, pair_range=(0, n_pairs))
+    r = O.bin_sums(data, pos, pop_rows, edges, genotypes=genotypes, max_dist=max_dist, pair_range=(0, n_pairs))
     return min(n_pairs, r["n_pairs"]), time.perf_counter() - t0
 
 
@@ -133,7 +133,7 @@ def cpu_sample_tasks(w, workers, pairs_per_worker):
         k = cand[t % len(cand)]
         a, b = int(offs[k]), int(offs[k + 1])
         tasks.append((np.ascontiguousarray(w.data[:, a:b]), w.positions[a:b].copy(), w.pop_rows, w.edges,
-                      w.max_dist, pairs_per_worker))
+                      w.max_dist, pairs_per_worker, bool(w.genotypes)))
     return tasks
 
 
@@ -189,9 +189,10 @@ def make_workload(cfg, scale, rank):
 
 
 def algorithmic_int_ops_per_pair(w):
-    """Count-stage INT ops per pair (MAC = 2): four 0/1 dot products of length n per
-    population with missing data (h.h, h.v, v.h, v.v), i.e. 8n per population."""
-    return sum(8 * len(r) for r in w.pop_rows)
+    """Count-stage INT ops per pair (MAC = 2): haplotypes, four 0/1 dot products of
+    length n per population (h.h, h.v, v.h, v.v), i.e. 8n; genotypes, the 3 x 3 Gram of
+    {g = 1, g = 2, valid}, i.e. 18n per population."""
+    return sum((18 if w.genotypes else 8) * len(r) for r in w.pop_rows)
 
 
 def main():
@@ -229,9 +230,9 @@ def main():
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = run_cpu_sample(w, args.cpu_seconds)
 
-    parser = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, method=args.method, max_dist=w.max_dist,
-                          window_offsets=w.window_offsets, snp_block=w.snp_block, n_blocks=w.n_blocks,
-                          device=dev)
+    parser = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, genotypes=w.genotypes, method=args.method,
+                          max_dist=w.max_dist, window_offsets=w.window_offsets, snp_block=w.snp_block,
+                          n_blocks=w.n_blocks, device=dev)
     reps_w = torch.as_tensor(w.replicate_weights if w.replicate_weights is not None
                              else np.ones((1, w.n_blocks), np.int32), dtype=torch.int32, device=dev)
     if w.window_of_block is not None:
@@ -327,9 +328,9 @@ def main():
     parity = None
     if args.method != "plain" and args.plain_steps > 0:
         fast = {k: v.copy() for k, v in parser.out.numpy().items()}
-        pp = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, method="plain", max_dist=w.max_dist,
-                          window_offsets=w.window_offsets, snp_block=w.snp_block, n_blocks=w.n_blocks,
-                          device=dev)
+        pp = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, genotypes=w.genotypes, method="plain",
+                          max_dist=w.max_dist, window_offsets=w.window_offsets, snp_block=w.snp_block,
+                          n_blocks=w.n_blocks, device=dev)
         pp.run()
         torch.cuda.synchronize()
         if ws > 1:
@@ -397,7 +398,10 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u8 counts / s32 accumulate / f64 estimators",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": {"tc": "u8 counts / s32 accumulate / f64 estimators",
+                      "tc32": "u8 counts / s32 accumulate / f32 estimators / f64 bin sums",
+                      "plain": "i8 byte counts / f64 estimators"}[args.method],
             "data": "synthetic (seeded founder mosaics; no public dataset offline)",
             "config": {"workload": w.name, "config_index": args.config, "scale": args.scale,
                        "snps": int(w.n_var), "pairs_per_step_per_gpu": int(n_pairs),
