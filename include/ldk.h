@@ -131,6 +131,24 @@ LDK_API int ldk_parse(const ldk_parse_t* d, const ldk_parse_out_t* out, void* wo
 #define LDK_NOALLOC_SCRATCH_BYTES (64ull << 20)
 LDK_API int ldk_parse_noalloc(const ldk_parse_t* d, const ldk_parse_out_t* out, void* stream);
 
+/* The parse split for CUDA-graph capture and repeated launches over one plan.  No
+ * counterpart in pg_gpu (its parse is a Python loop of CuPy calls).
+ *
+ * ldk_parse_setup writes the call's plan into the workspace -- window offsets and the
+ * tensor-core method's row-block list, from host memory -- and synchronises `stream`.
+ * ldk_parse_enqueue then enqueues only device work on `stream` (zeroing the outputs and
+ * the status word, pair ranges, indicator planes, the parse kernel): no host <-> device
+ * copies, no synchronisation, no allocation, so it can be captured into a CUDA graph and
+ * the graph replayed while the input arrays change contents in place.  It requires a
+ * preceding ldk_parse_setup with the same descriptor shape (n_var, populations, windows,
+ * method) and workspace.  ldk_parse_status synchronises `stream` and returns LDK_OK or
+ * LDK_ERR_DEVICE (with ldk_last_error) from the device status word the last enqueued
+ * parse on this workspace left.  ldk_parse = setup + enqueue + status. */
+LDK_API int ldk_parse_setup(const ldk_parse_t* d, void* workspace, size_t workspace_bytes, void* stream);
+LDK_API int ldk_parse_enqueue(const ldk_parse_t* d, const ldk_parse_out_t* out, void* workspace,
+                              size_t workspace_bytes, void* stream);
+LDK_API int ldk_parse_status(const void* workspace, void* stream);
+
 /* Per-thread kernel timing: while enabled, ldk_parse brackets its main counting /
  * estimator kernel with CUDA events on the caller's stream; ldk_profile_last_kernel_ms
  * returns that kernel's duration in the calling thread's last ldk_parse (-1 if none).

@@ -71,6 +71,10 @@ EXPORTS = {
     "ldk_parse": (ctypes.c_int, [ctypes.POINTER(ParseDesc), ctypes.POINTER(ParseOut), c_vp, ctypes.c_size_t,
                                  c_vp]),
     "ldk_parse_noalloc": (ctypes.c_int, [ctypes.POINTER(ParseDesc), ctypes.POINTER(ParseOut), c_vp]),
+    "ldk_parse_setup": (ctypes.c_int, [ctypes.POINTER(ParseDesc), c_vp, ctypes.c_size_t, c_vp]),
+    "ldk_parse_enqueue": (ctypes.c_int, [ctypes.POINTER(ParseDesc), ctypes.POINTER(ParseOut), c_vp,
+                                         ctypes.c_size_t, c_vp]),
+    "ldk_parse_status": (ctypes.c_int, [c_vp, c_vp]),
     "ldk_profile": (ctypes.c_int, [ctypes.c_int]),
     "ldk_profile_last_kernel_ms": (ctypes.c_double, []),
     "ldk_block_combine": (ctypes.c_int, [c_vp, ctypes.c_int64, ctypes.c_int64, c_vp, ctypes.c_int64, c_vp,

@@ -168,99 +168,124 @@ void set_error(const char* fmt, ...) {
 
 using namespace ldk;
 
-int ldk::parse_impl(const ldk_parse_t* d, const ldk_parse_out_t* out, void* workspace, size_t workspace_bytes,
-                    void* stream, bool device_items) {
-    if (int rc = validate(d)) return rc;
-    if (!out || !out->sums || !out->r2_sums || !out->pairs || !out->r2_counts) {
-        set_error("null output pointer");
-        return LDK_ERR_ARG;
-    }
+namespace ldk {
+namespace {
+
+// A parse call's geometry and its scratch carved out of the caller's workspace.
+struct Prepared {
     ParseShape sh;
-    shape_of(d, sh);
-    const Layout L = layout_of(d, sh);
-    if (!workspace || workspace_bytes < L.total) {
-        set_error("workspace of %zu bytes is smaller than the %zu required", workspace_bytes, L.total);
+    Layout L;
+    Scratch w;
+    unsigned char* ws = nullptr;
+};
+
+int prepare(const ldk_parse_t* d, void* workspace, size_t workspace_bytes, Prepared& P) {
+    if (int rc = validate(d)) return rc;
+    shape_of(d, P.sh);
+    P.L = layout_of(d, P.sh);
+    if (!workspace || workspace_bytes < P.L.total) {
+        set_error("workspace of %zu bytes is smaller than the %zu required", workspace_bytes, P.L.total);
         return LDK_ERR_WORKSPACE;
     }
     if (reinterpret_cast<uintptr_t>(workspace) % 256) { set_error("workspace must be 256-byte aligned"); return LDK_ERR_ARG; }
     if (int rc = check_arch()) return rc;
-    if (d->method != LDK_METHOD_PLAIN_FP64 && tc_smem_bytes(sh) > 227 * 1024) {
+    if (d->method != LDK_METHOD_PLAIN_FP64 && tc_smem_bytes(P.sh) > 227 * 1024) {
         set_error("bins x statistics exceed the tensor-core kernel's shared-memory staging");
         return LDK_ERR_UNSUPPORTED;
     }
-    cudaStream_t s = (cudaStream_t)stream;
     unsigned char* ws = static_cast<unsigned char*>(workspace);
-    Scratch w;
-    w.status = reinterpret_cast<unsigned*>(ws + L.status_off);
-    w.row_counter = reinterpret_cast<int*>(ws + L.status_off + 64);
-    w.item_counter = reinterpret_cast<int*>(ws + L.status_off + 128);
-    w.jmax = reinterpret_cast<int32_t*>(ws + L.jmax_off);
-    w.win_off = reinterpret_cast<int64_t*>(ws + L.win_off);
-    w.items = reinterpret_cast<int32_t*>(ws + L.items_off);
-    w.hv = ws + L.hv_off;
+    P.ws = ws;
+    P.w.status = reinterpret_cast<unsigned*>(ws + P.L.status_off);
+    P.w.row_counter = reinterpret_cast<int*>(ws + P.L.status_off + 64);
+    P.w.item_counter = reinterpret_cast<int*>(ws + P.L.status_off + 128);
+    P.w.jmax = reinterpret_cast<int32_t*>(ws + P.L.jmax_off);
+    P.w.win_off = reinterpret_cast<int64_t*>(ws + P.L.win_off);
+    P.w.items = reinterpret_cast<int32_t*>(ws + P.L.items_off);
+    P.w.hv = ws + P.L.hv_off;
+    return LDK_OK;
+}
 
+int check_outputs(const ldk_parse_out_t* out) {
+    if (!out || !out->sums || !out->r2_sums || !out->pairs || !out->r2_counts) {
+        set_error("null output pointer");
+        return LDK_ERR_ARG;
+    }
+    return LDK_OK;
+}
+
+// Host-side plan into the workspace: window offsets and, for the tensor-core method, the
+// row-block list (64 SNPs for haplotypes, 128 for genotypes, largest windows first; the
+// kernel's CTAs claim them in this order) -- or, with device_items, the list is built on
+// the device in window order.
+int upload_plan(const ldk_parse_t* d, const Prepared& P, cudaStream_t s, bool device_items) {
+    int rc;
+    std::vector<int64_t> woff(window_count(d) + 1);
+    for (int k = 0; k <= window_count(d); ++k) woff[k] = window_bound(d, k);
+    if ((rc = check_cuda(cudaMemcpyAsync(P.w.win_off, woff.data(), woff.size() * sizeof(int64_t),
+                                         cudaMemcpyHostToDevice, s), "upload windows")))
+        return rc;
+    if (d->method == LDK_METHOD_PLAIN_FP64) return LDK_OK;
+    const int rows = tc_rows_per_block(P.sh);
+    if (device_items)
+        return check_cuda(launch_build_items(P.w, window_count(d), rows, s), "row blocks");
+    std::vector<int> order(window_count(d));
+    for (int k = 0; k < (int)order.size(); ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        return (woff[x + 1] - woff[x]) > (woff[y + 1] - woff[y]);
+    });
+    std::vector<int32_t> items;
+    items.reserve((size_t)P.L.n_items * 2);
+    for (int wi : order)
+        for (int64_t r0 = woff[wi]; r0 < woff[wi + 1]; r0 += rows) {
+            items.push_back((int32_t)r0);
+            items.push_back((int32_t)std::min<int64_t>(r0 + rows, woff[wi + 1]));
+        }
+    if (!items.empty() &&
+        (rc = check_cuda(cudaMemcpyAsync(P.w.items, items.data(), items.size() * sizeof(int32_t),
+                                         cudaMemcpyHostToDevice, s), "upload row blocks")))
+        return rc;
+    return LDK_OK;
+}
+
+// Zeroes the outputs and the status block.
+int clear(const ldk_parse_t* d, const ldk_parse_out_t* out, const Prepared& P, cudaStream_t s) {
     const int nb = d->n_bins, NS = stats_of(d->n_pops);
     int rc;
     if ((rc = check_cuda(cudaMemsetAsync(out->sums, 0, sizeof(double) * d->n_blocks * nb * NS, s), "memset")) ||
         (rc = check_cuda(cudaMemsetAsync(out->r2_sums, 0, sizeof(double) * d->n_blocks * nb, s), "memset")) ||
         (rc = check_cuda(cudaMemsetAsync(out->pairs, 0, sizeof(uint64_t) * d->n_blocks * nb, s), "memset")) ||
         (rc = check_cuda(cudaMemsetAsync(out->r2_counts, 0, sizeof(uint64_t) * d->n_blocks * nb, s), "memset")) ||
-        (rc = check_cuda(cudaMemsetAsync(ws + L.status_off, 0, 256, s), "memset")))
+        (rc = check_cuda(cudaMemsetAsync(P.ws + P.L.status_off, 0, 256, s), "memset")))
         return rc;
-    if (d->n_var < 2) return LDK_OK;
+    return LDK_OK;
+}
 
-    std::vector<int64_t> woff(window_count(d) + 1);
-    for (int k = 0; k <= window_count(d); ++k) woff[k] = window_bound(d, k);
-    if ((rc = check_cuda(cudaMemcpyAsync(w.win_off, woff.data(), woff.size() * sizeof(int64_t),
-                                         cudaMemcpyHostToDevice, s), "upload windows")))
-        return rc;
+// Device work of one parse (after the plan is in the workspace): pair ranges, indicator
+// planes and the parse kernel.  Host work: tensor-map encoding and launch configuration.
+int enqueue_device(const ldk_parse_t* d, const ldk_parse_out_t* out, const Prepared& P, cudaStream_t s, bool prof) {
+    int rc;
     ldk_parse_t dd = *d;
     dd.n_windows = window_count(d);
-    if ((rc = check_cuda(launch_jmax(&dd, w, s), "pair ranges"))) return rc;
-
-    const bool prof = !device_items && g_prof && prof_events();
-    g_kernel_ms = -1.0f;
+    if ((rc = check_cuda(launch_jmax(&dd, P.w, s), "pair ranges"))) return rc;
     if (d->method == LDK_METHOD_PLAIN_FP64) {
         if (prof) cudaEventRecord(g_ev[0], s);
-        if ((rc = check_cuda(launch_parse_plain(&dd, out, w, sh, s), "plain parse"))) return rc;
+        if ((rc = check_cuda(launch_parse_plain(&dd, out, P.w, P.sh, s), "plain parse"))) return rc;
         if (prof) cudaEventRecord(g_ev[1], s);
     } else {
-        if (device_items) {
-            // row blocks in window order, listed on the device
-            if ((rc = check_cuda(launch_build_items(w, dd.n_windows, tc_rows_per_block(sh), s), "row blocks")))
-                return rc;
-        } else {
-            // row blocks (64 SNPs for haplotypes, 128 for genotypes), largest windows first;
-            // the kernel's CTAs claim them in this order
-            std::vector<int> order(window_count(d));
-            for (int k = 0; k < (int)order.size(); ++k) order[k] = k;
-            std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-                return (woff[x + 1] - woff[x]) > (woff[y + 1] - woff[y]);
-            });
-            std::vector<int32_t> items;
-            items.reserve((size_t)L.n_items * 2);
-            const int rows = tc_rows_per_block(sh);
-            for (int wi : order)
-                for (int64_t r0 = woff[wi]; r0 < woff[wi + 1]; r0 += rows) {
-                    items.push_back((int32_t)r0);
-                    items.push_back((int32_t)std::min<int64_t>(r0 + rows, woff[wi + 1]));
-                }
-            if (!items.empty() &&
-                (rc = check_cuda(cudaMemcpyAsync(w.items, items.data(), items.size() * sizeof(int32_t),
-                                                 cudaMemcpyHostToDevice, s), "upload row blocks")))
-                return rc;
-        }
-        if ((rc = check_cuda(launch_prep_planes(&dd, w, sh, s), "indicator planes"))) return rc;
+        if ((rc = check_cuda(launch_prep_planes(&dd, P.w, P.sh, s), "indicator planes"))) return rc;
         if (prof) cudaEventRecord(g_ev[0], s);
-        if ((rc = check_cuda(launch_parse_tc(&dd, out, w, sh, L.n_items, s), "tensor-core parse")))
-            return rc;
+        if ((rc = check_cuda(launch_parse_tc(&dd, out, P.w, P.sh, P.L.n_items, s), "tensor-core parse"))) return rc;
         if (prof) cudaEventRecord(g_ev[1], s);
     }
+    return LDK_OK;
+}
+
+int read_status(const unsigned* status_dev, cudaStream_t s) {
     unsigned status = 0;
-    if ((rc = check_cuda(cudaMemcpyAsync(&status, w.status, sizeof(unsigned), cudaMemcpyDeviceToHost, s), "status")))
+    int rc;
+    if ((rc = check_cuda(cudaMemcpyAsync(&status, status_dev, sizeof(unsigned), cudaMemcpyDeviceToHost, s), "status")))
         return rc;
     if ((rc = check_cuda(cudaStreamSynchronize(s), "ldk_parse"))) return rc;
-    if (prof) cudaEventElapsedTime(&g_kernel_ms, g_ev[0], g_ev[1]);
     if (status) {
         set_error("%s (status 0x%x)", status_text(status), status);
         return LDK_ERR_DEVICE;
@@ -268,7 +293,26 @@ int ldk::parse_impl(const ldk_parse_t* d, const ldk_parse_out_t* out, void* work
     return LDK_OK;
 }
 
+}  // namespace
+}  // namespace ldk
 
+int ldk::parse_impl(const ldk_parse_t* d, const ldk_parse_out_t* out, void* workspace, size_t workspace_bytes,
+                    void* stream, bool device_items) {
+    if (int rc = validate(d)) return rc;
+    if (int rc = check_outputs(out)) return rc;
+    Prepared P;
+    if (int rc = prepare(d, workspace, workspace_bytes, P)) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (int rc = clear(d, out, P, s)) return rc;
+    if (d->n_var < 2) return LDK_OK;
+    if (int rc = upload_plan(d, P, s, device_items)) return rc;
+    const bool prof = !device_items && g_prof && prof_events();
+    g_kernel_ms = -1.0f;
+    if (int rc = enqueue_device(d, out, P, s, prof)) return rc;
+    const int rc = read_status(P.w.status, s);
+    if (prof) cudaEventElapsedTime(&g_kernel_ms, g_ev[0], g_ev[1]);
+    return rc;
+}
 
 extern "C" {
 
@@ -341,6 +385,30 @@ size_t ldk_parse_workspace_size(const ldk_parse_t* d) {
 int ldk_parse(const ldk_parse_t* d, const ldk_parse_out_t* out, void* workspace, size_t workspace_bytes,
               void* stream) {
     return parse_impl(d, out, workspace, workspace_bytes, stream, false);
+}
+
+int ldk_parse_setup(const ldk_parse_t* d, void* workspace, size_t workspace_bytes, void* stream) {
+    Prepared P;
+    if (int rc = prepare(d, workspace, workspace_bytes, P)) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (int rc = upload_plan(d, P, s, false)) return rc;
+    return check_cuda(cudaStreamSynchronize(s), "ldk_parse_setup");
+}
+
+int ldk_parse_enqueue(const ldk_parse_t* d, const ldk_parse_out_t* out, void* workspace, size_t workspace_bytes,
+                      void* stream) {
+    if (int rc = check_outputs(out)) return rc;
+    Prepared P;
+    if (int rc = prepare(d, workspace, workspace_bytes, P)) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (int rc = clear(d, out, P, s)) return rc;
+    if (d->n_var < 2) return LDK_OK;
+    return enqueue_device(d, out, P, s, false);
+}
+
+int ldk_parse_status(const void* workspace, void* stream) {
+    if (!workspace) { set_error("null workspace"); return LDK_ERR_ARG; }
+    return read_status(static_cast<const unsigned*>(workspace), (cudaStream_t)stream);
 }
 
 int ldk_profile(int enable) {

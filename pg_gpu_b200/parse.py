@@ -136,6 +136,43 @@ class Parser:
         _lib.check(rc)
         return self.out
 
+    # -- the split form: plan once, enqueue device work only, read the status later
+    def setup(self, stream=None):
+        """Write the plan (window offsets, row blocks) into the workspace; synchronises."""
+        _lib.check(self.lib.ldk_parse_setup(ctypes.byref(self.desc), _lib.ptr(self.workspace),
+                                            self.workspace.numel(), _lib.stream_handle(stream)))
+
+    def enqueue(self, stream=None) -> ParseResult:
+        """Enqueue one parse (device work only; capturable).  Needs ``setup()`` first."""
+        _lib.check(self.lib.ldk_parse_enqueue(ctypes.byref(self.desc), ctypes.byref(self._o),
+                                              _lib.ptr(self.workspace), self.workspace.numel(),
+                                              _lib.stream_handle(stream)))
+        return self.out
+
+    def status(self, stream=None):
+        """Synchronise and raise LdkError if the last enqueued parse set a device error."""
+        _lib.check(self.lib.ldk_parse_status(_lib.ptr(self.workspace), _lib.stream_handle(stream)))
+
+    def graph(self, after=None):
+        """A CUDA graph of one parse (and of ``after(out)``, torch work on the outputs
+        whose result is returned beside the graph).  Replaying it re-reads the input
+        tensors (``self.X``, ``self.pos``, ...) in place; call ``status()`` after replays."""
+        torch = self.torch
+        self.setup()
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):  # warm-up outside the capture
+            out = self.enqueue()
+            if after is not None:
+                after(out)
+        torch.cuda.current_stream().wait_stream(side)
+        self.status()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            out = self.enqueue()
+            extra = after(out) if after is not None else None
+        return g, extra
+
 
 def ld_parse(data, positions, pop_rows, edges, **kw) -> ParseResult:
     """One-shot parse; see ``Parser`` for the arguments."""

@@ -328,3 +328,37 @@ def test_probe_peaks_plausible():
     assert 5e12 < f64 < 3e13, f64
     i8b, f64b = _lib.probe_peaks()
     assert abs(i8b - i8) < 0.2 * i8 and abs(f64b - f64) < 0.2 * f64
+
+
+@pytest.mark.parametrize("method", ["tc", "plain"])
+def test_parse_graph_replay_matches_run(method):
+    """Setup once, capture the enqueue in a CUDA graph, replay: same sums as ldk_parse;
+    after the input matrix changes in place, a replay matches a fresh parse of the new
+    data.  Two runs add the same FP64 terms in different atomic orders, so sums agree to
+    1e-11 relative (cancelling bins), pair tallies exactly."""
+    run_tol = 1e-11
+    w = synth.make_config(4, scale=0.003)
+    p = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, method=method, max_dist=w.max_dist,
+                     window_offsets=w.window_offsets, snp_block=w.snp_block, n_blocks=w.n_blocks)
+    want = {k: v.copy() for k, v in p.run().numpy().items()}
+    g, reps = p.graph(after=lambda out: parse.block_combine(out.sums, torch.ones((1, w.n_blocks), dtype=torch.int32,
+                                                                                   device="cuda")))
+    for _ in range(2):
+        g.replay()
+        p.status()
+        got = p.out.numpy()
+        np.testing.assert_array_equal(got["pairs"], want["pairs"])
+        assert rel_err(got["sums"], want["sums"], 1e-300) < run_tol
+        np.testing.assert_allclose(reps.cpu().numpy()[0], want["sums"].sum(axis=0), rtol=1e-11, atol=1e-12)
+    data2 = w.data.copy()
+    perm = np.random.default_rng(9).permutation(data2.shape[0])
+    data2[:, ::7] = data2[perm][:, ::7]  # re-pairs the haplotypes at every 7th SNP: new LD
+    p.X.copy_(torch.as_tensor(data2, device="cuda"))
+    g.replay()
+    p.status()
+    ref = parse.ld_parse(data2, w.positions, w.pop_rows, w.edges, method=method, max_dist=w.max_dist,
+                         window_offsets=w.window_offsets, snp_block=w.snp_block, n_blocks=w.n_blocks).numpy()
+    got = p.out.numpy()
+    np.testing.assert_array_equal(got["pairs"], ref["pairs"])
+    assert rel_err(got["sums"], ref["sums"], 1e-300) < run_tol
+    assert rel_err(got["sums"], want["sums"], 1e-300) > 1e-6  # the replay saw the new data
