@@ -149,6 +149,19 @@ LDK_API int ldk_parse_enqueue(const ldk_parse_t* d, const ldk_parse_out_t* out, 
                               size_t workspace_bytes, void* stream);
 LDK_API int ldk_parse_status(const void* workspace, void* stream);
 
+/* Tile autotuning of the tensor-core parse.  No counterpart in pg_gpu.  With enable = 1
+ * (or LDK_AUTOTUNE=1 in the environment at the first call), the first ldk_parse of each
+ * shape (population count, haplotype or genotype path, method, padded sample count) runs
+ * every candidate partner-tile width twice on its own input, times the second run of each
+ * with CUDA events,
+ * and keeps the fastest in a process-wide table (behind a mutex); that call returns the
+ * last candidate's sums (every candidate computes the same sums).  Later ldk_parse and
+ * ldk_parse_enqueue calls of the shape use the kept width; shapes never tuned use the
+ * default width.  ldk_tile_width returns the width (SNPs per partner tile) a call with
+ * this descriptor would use now, 0 for the plain method, or a negative status. */
+LDK_API int ldk_autotune(int enable);
+LDK_API int ldk_tile_width(const ldk_parse_t* d);
+
 /* Per-thread kernel timing: while enabled, ldk_parse brackets its main counting /
  * estimator kernel with CUDA events on the caller's stream; ldk_profile_last_kernel_ms
  * returns that kernel's duration in the calling thread's last ldk_parse (-1 if none).

@@ -75,6 +75,8 @@ EXPORTS = {
     "ldk_parse_enqueue": (ctypes.c_int, [ctypes.POINTER(ParseDesc), ctypes.POINTER(ParseOut), c_vp,
                                          ctypes.c_size_t, c_vp]),
     "ldk_parse_status": (ctypes.c_int, [c_vp, c_vp]),
+    "ldk_autotune": (ctypes.c_int, [ctypes.c_int]),
+    "ldk_tile_width": (ctypes.c_int, [ctypes.POINTER(ParseDesc)]),
     "ldk_profile": (ctypes.c_int, [ctypes.c_int]),
     "ldk_profile_last_kernel_ms": (ctypes.c_double, []),
     "ldk_block_combine": (ctypes.c_int, [c_vp, ctypes.c_int64, ctypes.c_int64, c_vp, ctypes.c_int64, c_vp,
@@ -138,3 +140,8 @@ def probe_peaks(stream=None):
     i8, f64 = ctypes.c_double(), ctypes.c_double()
     check(load().ldk_probe_peaks(ctypes.byref(i8), ctypes.byref(f64), stream_handle(stream)))
     return i8.value, f64.value
+
+
+def autotune(enable=True):
+    """Turn tile autotuning of the tensor-core parse on or off (``ldk_autotune``)."""
+    check(load().ldk_autotune(int(bool(enable))))

@@ -3,6 +3,10 @@
 #include <cstdio>
 #include <cstring>
 #include <algorithm>
+#include <array>
+#include <atomic>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "ldk_internal.h"
@@ -262,7 +266,46 @@ int clear(const ldk_parse_t* d, const ldk_parse_out_t* out, const Prepared& P, c
 
 // Device work of one parse (after the plan is in the workspace): pair ranges, indicator
 // planes and the parse kernel.  Host work: tensor-map encoding and launch configuration.
-int enqueue_device(const ldk_parse_t* d, const ldk_parse_out_t* out, const Prepared& P, cudaStream_t s, bool prof) {
+// ---- tile autotuning: the fastest tile variant per shape, process-wide behind a mutex
+std::atomic<int> g_autotune{-1};  // -1: LDK_AUTOTUNE not read yet
+std::mutex g_tune_mu;
+std::map<std::array<int, 4>, int> g_tuned;  // (populations, genotypes, method, K bytes) -> variant
+
+bool autotune_on() {
+    if (g_autotune.load() < 0) {
+        const char* e = getenv("LDK_AUTOTUNE");
+        int v = (e && atoi(e) == 1) ? 1 : 0, expect = -1;
+        g_autotune.compare_exchange_strong(expect, v);
+    }
+    return g_autotune.load() == 1;
+}
+
+std::array<int, 4> tune_key(const ldk_parse_t* d, const ParseShape& sh) {
+    return {sh.P, sh.genotypes, d->method, sh.ktot};
+}
+
+// The cached variant of this shape; -1 if the shape has not been tuned.
+int tuned_variant(const ldk_parse_t* d, const ParseShape& sh) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tuned.find(tune_key(d, sh));
+    return it == g_tuned.end() ? -1 : it->second;
+}
+
+// Tile variants worth timing: the alternative only where its width differs (the FP32
+// estimators have one variant).
+int n_variants(const ldk_parse_t* d, const ParseShape& sh) {
+    if (d->method == LDK_METHOD_TC_FP32) return 1;
+    return tc_tile_width(sh, 1) != tc_tile_width(sh, 0) ? 2 : 1;
+}
+
+// Runs every tile variant twice on this call's input (outputs cleared before each run) and
+// times the second run with CUDA events; caches the fastest.  The outputs keep the last
+// candidate's sums.
+int autotune_tc(const ldk_parse_t* dd, const ldk_parse_out_t* out, const Prepared& P, cudaStream_t s);
+int read_status(const unsigned* status_dev, cudaStream_t s);
+
+int enqueue_device(const ldk_parse_t* d, const ldk_parse_out_t* out, const Prepared& P, cudaStream_t s, bool prof,
+                   bool tune = false) {
     int rc;
     ldk_parse_t dd = *d;
     dd.n_windows = window_count(d);
@@ -273,10 +316,47 @@ int enqueue_device(const ldk_parse_t* d, const ldk_parse_out_t* out, const Prepa
         if (prof) cudaEventRecord(g_ev[1], s);
     } else {
         if ((rc = check_cuda(launch_prep_planes(&dd, P.w, P.sh, s), "indicator planes"))) return rc;
+        if (tune && n_variants(d, P.sh) > 1 && tuned_variant(d, P.sh) < 0)
+            if ((rc = autotune_tc(&dd, out, P, s))) return rc;
+        const int v = tuned_variant(d, P.sh);
         if (prof) cudaEventRecord(g_ev[0], s);
-        if ((rc = check_cuda(launch_parse_tc(&dd, out, P.w, P.sh, P.L.n_items, s), "tensor-core parse"))) return rc;
+        if ((rc = check_cuda(launch_parse_tc(&dd, out, P.w, P.sh, P.L.n_items, v < 0 ? 0 : v, s), "tensor-core parse")))
+            return rc;
         if (prof) cudaEventRecord(g_ev[1], s);
     }
+    return LDK_OK;
+}
+
+int autotune_tc(const ldk_parse_t* dd, const ldk_parse_out_t* out, const Prepared& P, cudaStream_t s) {
+    cudaEvent_t e0, e1;
+    int rc;
+    if ((rc = check_cuda(cudaEventCreate(&e0), "autotune events"))) return rc;
+    if ((rc = check_cuda(cudaEventCreate(&e1), "autotune events"))) { cudaEventDestroy(e0); return rc; }
+    float best_ms = 0.f;
+    int best = -1;
+    for (int v = 0; v < n_variants(dd, P.sh) && !rc; ++v) {
+        // an untimed run first (first-launch costs, caches), then the timed one
+        bool fits = true;
+        float ms = 0.f;
+        for (int rep = 0; rep < 2 && fits && !rc; ++rep) {
+            if ((rc = clear(dd, out, P, s))) break;
+            cudaEventRecord(e0, s);
+            if (launch_parse_tc(dd, out, P.w, P.sh, P.L.n_items, v, s) != cudaSuccess) {
+                cudaGetLastError();  // this variant does not fit the shape (e.g. shared memory): skip it
+                fits = false;
+                break;
+            }
+            cudaEventRecord(e1, s);
+            if ((rc = read_status(P.w.status, s))) break;
+            cudaEventElapsedTime(&ms, e0, e1);
+        }
+        if (fits && !rc && (best < 0 || ms < best_ms)) { best = v; best_ms = ms; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tuned[tune_key(dd, P.sh)] = best < 0 ? 0 : best;
     return LDK_OK;
 }
 
@@ -308,7 +388,7 @@ int ldk::parse_impl(const ldk_parse_t* d, const ldk_parse_out_t* out, void* work
     if (int rc = upload_plan(d, P, s, device_items)) return rc;
     const bool prof = !device_items && g_prof && prof_events();
     g_kernel_ms = -1.0f;
-    if (int rc = enqueue_device(d, out, P, s, prof)) return rc;
+    if (int rc = enqueue_device(d, out, P, s, prof, !device_items && autotune_on())) return rc;
     const int rc = read_status(P.w.status, s);
     if (prof) cudaEventElapsedTime(&g_kernel_ms, g_ev[0], g_ev[1]);
     return rc;
@@ -404,6 +484,20 @@ int ldk_parse_enqueue(const ldk_parse_t* d, const ldk_parse_out_t* out, void* wo
     if (int rc = clear(d, out, P, s)) return rc;
     if (d->n_var < 2) return LDK_OK;
     return enqueue_device(d, out, P, s, false);
+}
+
+int ldk_autotune(int enable) {
+    g_autotune.store(enable ? 1 : 0);
+    return LDK_OK;
+}
+
+int ldk_tile_width(const ldk_parse_t* d) {
+    if (int rc = validate(d)) return rc;
+    if (d->method == LDK_METHOD_PLAIN_FP64) return 0;
+    ParseShape sh;
+    shape_of(d, sh);
+    const int v = tuned_variant(d, sh);
+    return tc_tile_width(sh, v < 0 ? 0 : v);
 }
 
 int ldk_parse_status(const void* workspace, void* stream) {

@@ -136,6 +136,13 @@ class Parser:
         _lib.check(rc)
         return self.out
 
+    def tile_width(self):
+        """Partner SNPs per tile this parse uses now (tuned or default); 0 for "plain"."""
+        w = self.lib.ldk_tile_width(ctypes.byref(self.desc))
+        if w < 0:
+            _lib.check(w)
+        return w
+
     # -- the split form: plan once, enqueue device work only, read the status later
     def setup(self, stream=None):
         """Write the plan (window offsets, row blocks) into the workspace; synchronises."""

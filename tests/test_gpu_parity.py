@@ -362,3 +362,24 @@ def test_parse_graph_replay_matches_run(method):
     np.testing.assert_array_equal(got["pairs"], ref["pairs"])
     assert rel_err(got["sums"], ref["sums"], 1e-300) < run_tol
     assert rel_err(got["sums"], want["sums"], 1e-300) > 1e-6  # the replay saw the new data
+
+
+@pytest.mark.parametrize("genotypes", [False, True])
+def test_autotune_picks_a_candidate_and_keeps_results(genotypes):
+    """With tuning on, the first parse of a shape times the tile candidates and keeps one;
+    its results and those of later calls (tuned width) match the default-width parse."""
+    w = synth.make_config(3 if genotypes else 2, scale=0.01)
+    kw = dict(genotypes=w.genotypes, method="tc", max_dist=w.max_dist, window_offsets=w.window_offsets,
+              snp_block=w.snp_block, n_blocks=w.n_blocks)
+    ref = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, **kw)
+    want = {k: v.copy() for k, v in ref.run().numpy().items()}
+    try:
+        _lib.autotune(True)
+        p = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, **kw)
+        for _ in range(2):
+            got = p.run().numpy()
+            np.testing.assert_array_equal(got["pairs"], want["pairs"])
+            assert rel_err(got["sums"], want["sums"], 1e-300) < 1e-11
+        assert p.tile_width() in ({16, 8} if genotypes else {64, 32})
+    finally:
+        _lib.autotune(False)
