@@ -821,3 +821,149 @@ def geno_biallelic_keep(geno, rows_union=None):
     alt = np.where(v, g, 0).astype(np.int64).sum(axis=0)
     nv = v.sum(axis=0)
     return (alt > 0) & (alt < 2 * nv) & (nv >= 2)
+
+
+# ---------------------------------------------------------------------------
+# all-pairs LD of one SNP set: pairwise r^2, sigma_D^2, r^2 from joint counts, ZnS, Omega,
+# windowed r^2 percentiles  (haplotype_matrix.py:1092-1317, ld_statistics.py:249-862)
+# ---------------------------------------------------------------------------
+
+
+def segregating(hap, missing_data="include"):
+    """Column indices kept by ``_prepare_segregating`` (ld_statistics.py:249-278):
+    with 'exclude' only sites without missing calls, then sites with 0 < dac < n_valid."""
+    hap = np.asarray(hap)
+    keep = np.arange(hap.shape[1])
+    if missing_data == "exclude":
+        keep = keep[np.sum(hap < 0, axis=0) == 0]
+    sub = hap[:, keep]
+    dac = np.maximum(sub, 0).sum(axis=0)
+    nv = (sub >= 0).sum(axis=0)
+    return keep[(dac > 0) & (dac < nv)]
+
+
+def _gram_counts(hap):
+    """c1..c4 and n (joint valid) for all column pairs (ld_statistics.py:281-299)."""
+    v = (hap >= 0).astype(np.float64)
+    h = np.where(hap >= 0, hap, 0).astype(np.float64)
+    c1 = h.T @ h
+    s12 = h.T @ v
+    s13 = v.T @ h
+    n = v.T @ v
+    return c1, s12 - c1, s13 - c1, n - s12 - s13 + c1, n
+
+
+def pairwise_r2_matrix(hap):
+    """``HaplotypeMatrix.pairwise_r2('r2')`` (haplotype_matrix.py:1092-1136, 1171-1175):
+    D = p_AB - p_i p_j with p_AB over jointly valid haplotypes and p_i over the site's valid
+    haplotypes; r^2 = D^2 / (p_i q_i p_j q_j), 0 where that product is 0; diagonal 0."""
+    hap = np.asarray(hap)
+    v = (hap >= 0).astype(np.float64)
+    h = np.where(hap >= 0, hap, 0).astype(np.float64)
+    nv = v.sum(axis=0)
+    p = np.where(nv > 0, h.sum(axis=0) / np.where(nv > 0, nv, 1), 0.0)
+    jn = v.T @ v
+    j11 = h.T @ h
+    pab = np.where(jn > 0, j11 / np.where(jn > 0, jn, 1), 0.0)
+    D = pab - np.outer(p, p)
+    den = np.outer(p * (1 - p), p * (1 - p))
+    r2 = np.where(den > 0, D ** 2 / np.where(den > 0, den, 1), 0.0)
+    np.fill_diagonal(r2, 0.0)
+    return r2
+
+
+def sigma_d2_matrix(hap):
+    """Unbiased sigma_D^2 = D^2 / pi2 numerators per pair (ld_statistics.py:311-344,
+    788-810): 0 where n < 4 or the pi2 numerator is 0; diagonal 0.  Also returns the
+    valid mask n >= 4 (diagonal False) that ZnS counts."""
+    c1, c2, c3, c4, n = _gram_counts(np.asarray(hap))
+    dd = c1 * (c1 - 1) * c4 * (c4 - 1) + c2 * (c2 - 1) * c3 * (c3 - 1) - 2 * c1 * c2 * c3 * c4
+    s12, s13, s24, s34 = c1 + c2, c1 + c3, c2 + c4, c3 + c4
+    pi2 = (s12 * s13 * s24 * s34 - c1 * c4 * (-1 + c1 + 3 * c2 + 3 * c3 + c4)
+           - c2 * c3 * (-1 + 3 * c1 + c2 + c3 + 3 * c4))
+    valid = n >= 4
+    out = np.where(valid & (pi2 != 0), dd / np.where(pi2 != 0, pi2, 1), 0.0)
+    np.fill_diagonal(out, 0.0)
+    np.fill_diagonal(valid, False)
+    return out, valid
+
+
+def r2_counts_matrix(hap):
+    """r^2 from the jointly valid two-locus counts for every pair, the estimator of
+    ``ld_statistics.r_squared`` (haplotype_kernels.py:32-42) that ``windowed_r_squared``
+    applies to every pair (haplotype_matrix.py:1285-1289): NaN where pA qA pB qB = 0;
+    diagonal NaN."""
+    c1, c2, c3, c4, n = _gram_counts(np.asarray(hap))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        D = c1 * c4 - c2 * c3
+        den = (c1 + c2) * (c3 + c4) * (c1 + c3) * (c2 + c4)
+        r2 = np.where(den > 0, D * D / np.where(den > 0, den, 1), np.nan)
+    np.fill_diagonal(r2, np.nan)
+    return r2
+
+
+def zns(hap, estimator="sigma_d2", missing_data="include"):
+    """Kelly's ZnS on segregating sites (ld_statistics.py:534-596, 679-718): mean naive
+    pairwise r^2 over the m(m-1)/2 pairs, or mean sigma_D^2 over pairs with n >= 4.  With
+    the sigma_D^2 estimator the reference replaces ``missing_data`` by its internal
+    projection mode (ld_statistics.py:711), so 'exclude' is not applied there."""
+    if estimator != "r2":
+        missing_data = "include"
+    sub = np.asarray(hap)[:, segregating(hap, missing_data)]
+    m = sub.shape[1]
+    if m < 2:
+        return 0.0
+    if estimator == "r2":
+        r2 = pairwise_r2_matrix(sub)
+        return float(r2.sum() / (m * (m - 1)))
+    sd, valid = sigma_d2_matrix(sub)
+    npairs = int(valid.sum())
+    return float(sd.sum() / npairs) if npairs > 0 else 0.0
+
+
+def omega(hap, estimator="sigma_d2", missing_data="include"):
+    """Kim & Nielsen's Omega on segregating sites (ld_statistics.py:761-862): max over
+    split points l = 3 .. m-2 of mean within-block / mean cross-block value, upper
+    triangle pairs only; 0 if fewer than 5 sites."""
+    sub = np.asarray(hap)[:, segregating(hap, missing_data)]
+    m = sub.shape[1]
+    if m < 5:
+        return 0.0
+    mat = pairwise_r2_matrix(sub) if estimator == "r2" else sigma_d2_matrix(sub)[0]
+    up = np.triu(mat, k=1)
+    best = 0.0
+    for l in range(3, m - 1):
+        left = up[:l, :l].sum()
+        cross = up[:l, l:].sum()
+        right = up[l:, l:].sum()
+        n_within = l * (l - 1) // 2 + (m - l) * (m - l - 1) // 2
+        n_cross = l * (m - l)
+        if n_within > 0 and n_cross > 0 and cross > 0:
+            best = max(best, ((left + right) / n_within) / (cross / n_cross))
+    return float(best)
+
+
+def windowed_r2(hap, positions, bp_bins, percentile=50):
+    """``HaplotypeMatrix.windowed_r_squared`` with the 'r2' estimator
+    (haplotype_matrix.py:1235-1317): r^2 from joint counts for every pair i < j, binned by
+    pos[j] - pos[i] with digitize (right-open), NaN pairs dropped; per-bin percentiles
+    (NaN for empty bins) and pair counts."""
+    r2 = r2_counts_matrix(hap)
+    pos = np.asarray(positions)
+    m = len(pos)
+    iu, ju = np.triu_indices(m, k=1)
+    vals = r2[iu, ju]
+    dist = pos[ju] - pos[iu]
+    edges = np.asarray(bp_bins)
+    nb = len(edges) - 1
+    b = np.digitize(dist, edges) - 1
+    ok = (b >= 0) & (b < nb) & ~np.isnan(vals)
+    pct = np.atleast_1d(percentile)
+    res = np.full((nb, len(pct)), np.nan)
+    cnt = np.zeros(nb, dtype=int)
+    for k in range(nb):
+        sel = vals[ok & (b == k)]
+        cnt[k] = len(sel)
+        if len(sel):
+            res[k] = np.percentile(sel, pct)
+    return (res[:, 0] if res.shape[1] == 1 else res), cnt

@@ -7,6 +7,8 @@ fixtures it writes are committed and are all the tests need elsewhere.
   + ``im_pop.txt``) read into the HaplotypeMatrix layout (``haplotype_matrix.py:326-329``,
   populations as rows i and i + n_samples, ``:509-510``) together with moments' own output
   cached by the reference (``tests/cache/moments_ld_test_im_4bins_deme0-deme1.pkl``).
+* ``ref_ldm.npz`` -- the reference's all-pairs LD functions (pairwise r^2, sigma_D^2
+  matrix, ZnS, Omega, windowed r^2 percentiles) on seeded haplotypes.
 * ``ref_*.npz`` / ``ref_names.json`` -- outputs of the reference's own functions
   (``ld_pipeline``, ``ld_statistics``, ``haplotype_kernels``, ``genotype_kernels``,
   ``ld_statistics_genotype``), run on the CPU via ``oracle/ref_shim.py`` with the
@@ -196,6 +198,63 @@ def make_reference_fixtures(reference):
     np.savez_compressed(os.path.join(HERE, "ref_geno.npz"), **geno_out)
 
 
+def make_ldm_fixtures(reference):
+    """``ref_ldm.npz``: the reference's all-pairs LD functions -- HaplotypeMatrix.pairwise_r2,
+    ld_statistics._build_sigma_d2_matrix, zns, omega, HaplotypeMatrix.windowed_r_squared --
+    on seeded haplotypes with missing calls and monomorphic sites.  haplotype_matrix.py
+    imports scikit-allel / tskit / zarr at module level; stand-in modules satisfy those
+    imports (none of the functions used here touches them), and the NumPy-backed cupy
+    stand-in gets a ``.get()`` on reduction results."""
+    import types
+
+    class _Stub(types.ModuleType):
+        def __getattr__(self, k):
+            return type(k, (), {})
+
+    for name in ("allel", "tskit", "zarr", "msprime", "moments"):
+        sys.modules.setdefault(name, _Stub(name))
+    mods = ref_shim.import_reference_modules(reference, ["ld_statistics", "haplotype_matrix"])
+
+    class _A(np.ndarray):
+        def get(self):
+            return np.asarray(self)
+
+    cpm = sys.modules["cupy"]
+    for fn in ("sum", "max", "trace", "digitize"):
+        f = getattr(np, fn)
+        setattr(cpm, fn, (lambda f: lambda *a, **k: np.asarray(f(*a, **k)).view(_A))(f))
+    L = mods["ld_statistics"]
+    rs = L.r_squared
+    L.r_squared = lambda *a, **k: np.asarray(rs(*a, **k)).view(_A)
+    HM = mods["haplotype_matrix"].HaplotypeMatrix
+
+    rng = np.random.default_rng(77)
+    n_hap, m = 64, 90
+    founders = (rng.random((5, m)) < rng.uniform(0.05, 0.7, m)).astype(np.int8)
+    hap = founders[rng.integers(0, 5, n_hap)]
+    hap = np.where(rng.random(hap.shape) < 0.04, 1 - hap, hap).astype(np.int8)
+    hap[:, 7] = 0                                  # monomorphic
+    hap[:, 30] = 1                                 # monomorphic (derived everywhere)
+    hap[rng.random(hap.shape) < 0.05] = -1         # missing calls
+    pos = np.sort(rng.choice(200_000, m, replace=False)).astype(np.int64)
+    out = {"hap": hap, "pos": pos}
+    hm = HM(hap.copy(), pos.copy())
+    out["pairwise_r2"] = np.asarray(hm.pairwise_r2())
+    out["sigma_d2_seg"] = np.asarray(L._build_sigma_d2_matrix(HM(hap.copy(), pos.copy())))
+    for md in ("include", "exclude"):
+        for est in ("r2", "sigma_d2"):
+            out[f"zns_{est}_{md}"] = np.float64(L.zns(HM(hap.copy(), pos.copy()), missing_data=md, estimator=est))
+            out[f"omega_{est}_{md}"] = np.float64(L.omega(HM(hap.copy(), pos.copy()), missing_data=md,
+                                                          estimator=est))
+    for k, (bins, pct) in enumerate((([0, 1000, 5000, 20000, 200000], [10, 50, 95]), ([0, 50000, 200000], 50))):
+        res, cnt = HM(hap.copy(), pos.copy()).windowed_r_squared(np.array(bins), percentile=pct)
+        out[f"win{k}_bins"] = np.array(bins, dtype=np.float64)
+        out[f"win{k}_pct"] = np.atleast_1d(pct).astype(np.float64)
+        out[f"win{k}_res"] = np.asarray(res)
+        out[f"win{k}_cnt"] = np.asarray(cnt)
+    np.savez_compressed(os.path.join(HERE, "ref_ldm.npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=build_ref.DEFAULT_REFERENCE)
@@ -203,6 +262,7 @@ def main():
     build_ref.build(args.reference)
     make_im_example(args.reference)
     make_reference_fixtures(args.reference)
+    make_ldm_fixtures(args.reference)
     for f in sorted(os.listdir(HERE)):
         if f.endswith((".npz", ".json")):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -149,3 +149,22 @@ def test_bin_semantics_right_open():
     edges = [10.0, 100.0, 1000.0]
     d = np.array([5.0, 10.0, 99.9, 100.0, 999.0, 1000.0, 2000.0])
     np.testing.assert_array_equal(O.bin_index(d, edges), [-1, 0, 0, 1, 1, 2, 2])
+
+
+def test_all_pairs_ld_oracle_matches_reference(golden_dir):
+    """pairwise r^2, sigma_D^2 matrix, ZnS, Omega and windowed r^2 percentiles of the
+    oracle against the reference's own functions (tests/golden/ref_ldm.npz)."""
+    g = np.load(os.path.join(golden_dir, "ref_ldm.npz"))
+    hap, pos = g["hap"], g["pos"]
+    np.testing.assert_allclose(O.pairwise_r2_matrix(hap), g["pairwise_r2"], rtol=1e-12, atol=1e-15)
+    seg = O.segregating(hap)
+    np.testing.assert_allclose(O.sigma_d2_matrix(hap[:, seg])[0], g["sigma_d2_seg"], rtol=1e-12, atol=1e-15)
+    for md in ("include", "exclude"):
+        for est in ("r2", "sigma_d2"):
+            np.testing.assert_allclose(O.zns(hap, est, md), g[f"zns_{est}_{md}"], rtol=1e-12, atol=1e-15)
+            np.testing.assert_allclose(O.omega(hap, est, md), g[f"omega_{est}_{md}"], rtol=1e-12, atol=1e-15)
+    for k in range(2):
+        pct = g[f"win{k}_pct"]
+        res, cnt = O.windowed_r2(hap, pos, g[f"win{k}_bins"], pct if len(pct) > 1 else pct[0])
+        np.testing.assert_array_equal(cnt, g[f"win{k}_cnt"])
+        np.testing.assert_allclose(res, g[f"win{k}_res"], rtol=1e-12, equal_nan=True)
