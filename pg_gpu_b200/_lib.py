@@ -76,6 +76,9 @@ EXPORTS = {
                                          ctypes.c_size_t, c_vp]),
     "ldk_parse_status": (ctypes.c_int, [c_vp, c_vp]),
     "ldk_autotune": (ctypes.c_int, [ctypes.c_int]),
+    "ldk_ld_matrix_workspace_size": (ctypes.c_size_t, [ctypes.c_int64, ctypes.c_int32]),
+    "ldk_ld_matrix": (ctypes.c_int, [c_vp, ctypes.c_int64, ctypes.c_int64, c_vp, ctypes.c_int32, ctypes.c_int, c_vp,
+                                     ctypes.c_int64, c_vp, c_vp, ctypes.c_size_t, c_vp]),
     "ldk_tile_width": (ctypes.c_int, [ctypes.POINTER(ParseDesc)]),
     "ldk_profile": (ctypes.c_int, [ctypes.c_int]),
     "ldk_profile_last_kernel_ms": (ctypes.c_double, []),

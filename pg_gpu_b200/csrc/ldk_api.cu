@@ -486,6 +486,37 @@ int ldk_parse_enqueue(const ldk_parse_t* d, const ldk_parse_out_t* out, void* wo
     return enqueue_device(d, out, P, s, false);
 }
 
+size_t ldk_ld_matrix_workspace_size(int64_t n_var, int32_t n_sel) {
+    if (n_var < 0 || n_sel < 1) return 0;
+    return ld_matrix_workspace(n_var, n_sel);
+}
+
+int ldk_ld_matrix(const int8_t* X, int64_t ld_x, int64_t n_var, const int32_t* rows, int32_t n_sel, int estimator,
+                  double* out, int64_t ld_out, double* sums, void* workspace, size_t workspace_bytes, void* stream) {
+    if (n_var < 0 || n_var > (int64_t)INT32_MAX - 1024 || n_sel < 1 || ld_x < n_var) {
+        set_error("bad sizes");
+        return LDK_ERR_ARG;
+    }
+    if (estimator < LDK_LDM_R2 || estimator > LDK_LDM_R2_COUNTS) { set_error("unknown estimator"); return LDK_ERR_ARG; }
+    if (n_var > 0 && (!X || !rows)) { set_error("null input pointer"); return LDK_ERR_ARG; }
+    if (out && ld_out < n_var) { set_error("ld_out < n_var"); return LDK_ERR_ARG; }
+    const size_t need = ld_matrix_workspace(n_var, n_sel);
+    if (!workspace || workspace_bytes < need) {
+        set_error("workspace of %zu bytes is smaller than the %zu required", workspace_bytes, need);
+        return LDK_ERR_WORKSPACE;
+    }
+    if (reinterpret_cast<uintptr_t>(workspace) % 256) { set_error("workspace must be 256-byte aligned"); return LDK_ERR_ARG; }
+    if (int rc = check_arch()) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned char* ws = static_cast<unsigned char*>(workspace);
+    unsigned* status = reinterpret_cast<unsigned*>(ws);
+    if (int rc = check_cuda(cudaMemsetAsync(ws, 0, 256, s), "memset")) return rc;
+    if (int rc = check_cuda(launch_ld_matrix(X, ld_x, n_var, rows, n_sel, estimator, out, ld_out, sums, ws, status, s),
+                            "all-pairs LD"))
+        return rc;
+    return read_status(status, s);
+}
+
 int ldk_autotune(int enable) {
     g_autotune.store(enable ? 1 : 0);
     return LDK_OK;

@@ -66,6 +66,12 @@ size_t tc_smem_bytes(const ParseShape& sh);
 
 cudaError_t launch_build_items(const Scratch& w, int n_windows, int rows, cudaStream_t s);
 
+// all-pairs LD of one SNP set (ldk_ldm.cu)
+size_t ld_matrix_workspace(int64_t n_var, int32_t n_sel);
+cudaError_t launch_ld_matrix(const int8_t* X, int64_t ld_x, int64_t n_var, const int32_t* rows, int32_t n_sel,
+                             int estimator, double* out, int64_t ld_out, double* sums, unsigned char* ws,
+                             unsigned* status, cudaStream_t s);
+
 // ldk_parse with a caller-provided workspace; device_items lists the tensor-core row
 // blocks with a device kernel (window order) instead of a host-built upload.
 int parse_impl(const ldk_parse_t* d, const ldk_parse_out_t* out, void* workspace, size_t workspace_bytes,

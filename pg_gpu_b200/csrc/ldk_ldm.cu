@@ -1,0 +1,352 @@
+// All-pairs LD of one SNP set on the tensor-core count pipeline: pairwise r^2, the
+// unbiased sigma_D^2 and r^2 from jointly valid counts for every pair i < j, written as a
+// full symmetric matrix and/or reduced to the sum and count behind ZnS.
+//
+// The Gram counts come from the same TMA + tcgen05 pipeline as the binned parse (64-SNP
+// row blocks against 128-SNP partner tiles, no distance cutoff, so every partner j > i of
+// the set).  Each epilogue warp evaluates its 16 rows x 128 partners of a tile into a
+// padded shared-memory tile and then writes the tile's rows (upper triangle, 1 KB runs)
+// and columns (lower triangle, 128-byte runs) with coalesced stores: the kernel is bound
+// by the n^2 x 8 bytes it writes.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "ldk_tc_kernel.cuh"
+
+namespace ldk {
+
+namespace {
+
+using LdmCfg = Cfg<1, false, 0>;
+constexpr int kLdmStride = LdmCfg::NJ + 1;  // staging row stride (doubles): rows hit distinct banks
+
+struct LdmArgs {
+    const double* psite;  // per SNP: derived allele frequency over the site's valid haplotypes
+    double* out;          // (n_var rows, stride ld_out) or null
+    int64_t ld_out;
+    double* sums;         // [sum over pairs i < j, pairs counted] or null
+};
+
+__global__ void k_fill_int(int32_t* p, int64_t n, int32_t v) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        p[t] = v;
+}
+
+__global__ void k_fill_diag(double* out, int64_t ld, int64_t n, double v) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        out[t * ld + t] = v;
+}
+
+// p_i = (sum of derived calls) / (valid calls), 0 for a site without valid calls
+// (haplotype_matrix.py:1119-1120), over the selected rows.
+__global__ void k_site_freq(const int8_t* __restrict__ X, int64_t ld, int64_t n_var, const int32_t* __restrict__ rows,
+                            int n_rows, double* __restrict__ p) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n_var; v += (int64_t)gridDim.x * blockDim.x) {
+        int dac = 0, nv = 0;
+        for (int k = 0; k < n_rows; ++k) {
+            const int8_t x = X[(int64_t)rows[k] * ld + v];
+            dac += x > 0 ? x : 0;
+            nv += x >= 0;
+        }
+        p[v] = nv > 0 ? (double)dac / (double)nv : 0.0;
+    }
+}
+
+template <int EST>
+__global__ void __launch_bounds__(128 + 32 * kEpi, 1)
+    k_ld_matrix(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcArgs a,
+                const LdmArgs m) {
+    using C = LdmCfg;
+    constexpr int NJ = C::NJ, SP = kLdmStride;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char* stages = base;
+    double* stile = reinterpret_cast<double*>(base + C::STAGES * C::STAGE_BYTES);  // [kEpi][16][SP]
+
+    __shared__ __align__(8) uint64_t full_bar[C::STAGES], empty_bar[C::STAGES], tfull[C::NBUF], tempty[C::NBUF];
+    __shared__ __align__(8) uint64_t ifull[kRing], iempty[kRing];
+    __shared__ volatile int ring[kRing];
+    __shared__ uint32_t tmem_base_s;
+    __shared__ volatile int abort_s;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < C::STAGES; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], 1);
+        }
+        for (int b = 0; b < C::NBUF; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], kEpi);
+        }
+        for (int b = 0; b < kRing; ++b) {
+            mbar_init(&ifull[b], 1);
+            mbar_init(&iempty[b], 1 + kEpi);
+        }
+        abort_s = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        tmem_alloc(&tmem_base_s, kTmemCols);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base_s;
+    const Pipe pipe{stages, full_bar, empty_bar, tfull, tempty, ifull, iempty, ring, &abort_s};
+    if (warp == 0) run_producer<C>(pipe, &tmA, &tmB, a, lane);
+    else if (warp == 1) run_mma<C, 1>(pipe, tmem, a, lane);
+    if (warp >= 4) {
+        // lanes 2r, 2r+1 share SNP r (16 per warp) and split its partners by parity
+        const int e = warp - 4, quarter = warp & 3;
+        const int rr = lane >> 1, role = lane & 1;
+        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+        double* st = stile + e * 16 * SP;
+        double zsum = 0.0, zcnt = 0.0;
+        uint32_t tcount = 0;
+        for (uint32_t k = 0;; ++k) {
+            const int sl = k % kRing;
+            int item = -1;
+            if (lane == 0) {
+                if (mbar_wait(&ifull[sl], (k / kRing) & 1u, &abort_s, a.status)) {
+                    item = ring[sl];
+                    mbar_arrive(&iempty[sl]);
+                }
+            }
+            item = __shfl_sync(0xffffffffu, item, 0);
+            if (epi_bar_or<kEpi>(abort_s != 0 || item < 0)) break;
+            const int row0 = a.items[2 * item], row1 = a.items[2 * item + 1];
+            const int jend = a.jmax[row1 - 1];
+            const int n_jt = jend > row0 + 1 ? (jend - row0 + NJ - 1) / NJ : 0;
+            if (n_jt == 0) continue;
+            const int i = row0 + quarter * 16 + rr;
+            const bool row_ok = i < row1;
+            const double pi = (EST == 0 && row_ok) ? m.psite[i] : 0.0;
+            bool ok = true;
+            for (int t = 0; t < n_jt; ++t, ++tcount) {
+                const uint32_t buf = tcount % C::NBUF, tph = (tcount / C::NBUF) & 1u;
+                const int j0 = row0 + t * NJ;
+                double preg[NJ / 32];
+#pragma unroll
+                for (int kk = 0; kk < NJ / 32; ++kk) {
+                    const int j = j0 + 32 * kk + lane;
+                    preg[kk] = (EST == 0 && j < jend) ? m.psite[j] : 0.0;
+                }
+                if (!mbar_wait(&tfull[buf], tph, &abort_s, a.status)) { ok = false; break; }
+                tc_fence_after();
+#pragma unroll 1
+                for (int q = 0; q < NJ / 2; ++q) {
+                    uint32_t v[1][4];
+                    tmem_ld4(tmem + lane_base + buf * C::COLS + q * 4, v[0]);
+                    const int jj = 2 * q + role;
+                    double psrc = preg[0];
+#pragma unroll
+                    for (int kk = 1; kk < NJ / 32; ++kk)
+                        if ((jj >> 5) == kk) psrc = preg[kk];
+                    const double pj = __shfl_sync(0xffffffffu, psrc, jj & 31);
+                    tmem_wait4<1>(v);
+                    if (q == NJ / 2 - 1) {
+                        tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(&tempty[buf]);
+                    }
+                    // lane 2r: (hh, hv) of partners 2q, 2q+1; lane 2r+1: (vh, vv)
+                    const uint32_t sx = role ? v[0][0] : v[0][2];
+                    const uint32_t sy = role ? v[0][1] : v[0][3];
+                    const uint32_t rx = __shfl_xor_sync(0xffffffffu, sx, 1);
+                    const uint32_t ry = __shfl_xor_sync(0xffffffffu, sy, 1);
+                    int hh, hv, vh, vv;
+                    if (role == 0) { hh = (int)v[0][0]; hv = (int)v[0][1]; vh = (int)rx; vv = (int)ry; }
+                    else { vh = (int)v[0][2]; vv = (int)v[0][3]; hh = (int)rx; hv = (int)ry; }
+                    const int j = j0 + jj;
+                    const bool valid = row_ok && j > i && j < jend;
+                    double val = 0.0;
+                    if (valid) {
+                        const double c1 = hh, c2 = hv - hh, c3 = vh - hh, c4 = vv - hv - vh + hh, n = vv;
+                        if constexpr (EST == 0) {
+                            // haplotype_matrix.py:1122-1128, 1171-1175
+                            const double pab = n > 0.0 ? c1 / n : 0.0;
+                            const double D = pab - pi * pj;
+                            const double den = (pi * (1.0 - pi)) * (pj * (1.0 - pj));
+                            val = den > 0.0 ? D * D / den : 0.0;
+                            zsum += val;
+                            zcnt += 1.0;
+                        } else if constexpr (EST == 1) {
+                            // ld_statistics.py:326-343 (exact integers in FP64)
+                            const double dd = c1 * (c1 - 1) * c4 * (c4 - 1) + c2 * (c2 - 1) * c3 * (c3 - 1) -
+                                              2.0 * c1 * c2 * c3 * c4;
+                            const double s12 = c1 + c2, s13 = c1 + c3, s24 = c2 + c4, s34 = c3 + c4;
+                            const double pi2 = s12 * s13 * s24 * s34 - c1 * c4 * (-1.0 + c1 + 3.0 * c2 + 3.0 * c3 + c4) -
+                                               c2 * c3 * (-1.0 + 3.0 * c1 + c2 + c3 + 3.0 * c4);
+                            const bool nok = n >= 4.0;
+                            val = (nok && pi2 != 0.0) ? dd / pi2 : 0.0;
+                            zsum += val;
+                            zcnt += nok ? 1.0 : 0.0;
+                        } else {
+                            // haplotype_kernels.py:32-42: NaN where pA qA pB qB = 0
+                            const double D = c1 * c4 - c2 * c3;
+                            const double den = (c1 + c2) * (c3 + c4) * ((c1 + c3) * (c2 + c4));
+                            if (den > 0.0) {
+                                val = D * D / den;
+                                zsum += val;
+                                zcnt += 1.0;
+                            } else {
+                                val = CUDART_NAN;
+                            }
+                        }
+                    }
+                    st[rr * SP + jj] = val;
+                }
+                __syncwarp();
+                if (m.out) {
+                    const int gi0 = row0 + quarter * 16;
+                    for (int idx = lane; idx < 16 * NJ; idx += 32) {  // rows: upper triangle
+                        const int r = idx / NJ, c = idx % NJ, gi = gi0 + r, gj = j0 + c;
+                        if (gi < row1 && gj > gi && gj < jend) m.out[(int64_t)gi * m.ld_out + gj] = st[r * SP + c];
+                    }
+                    for (int idx = lane; idx < 16 * NJ; idx += 32) {  // columns: lower triangle
+                        const int r = idx % 16, c = idx / 16, gi = gi0 + r, gj = j0 + c;
+                        if (gi < row1 && gj > gi && gj < jend) m.out[(int64_t)gj * m.ld_out + gi] = st[r * SP + c];
+                    }
+                }
+                __syncwarp();
+            }
+            (void)ok;
+        }
+        if (m.sums) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                zsum += __shfl_xor_sync(0xffffffffu, zsum, o);
+                zcnt += __shfl_xor_sync(0xffffffffu, zcnt, o);
+            }
+            if (lane == 0) {
+                atomicAdd(&m.sums[0], zsum);
+                atomicAdd(&m.sums[1], zcnt);
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem, kTmemCols);
+    }
+}
+
+struct LdmLayout {
+    size_t status = 0, jmax = 0, items = 0, planes = 0, psite = 0, total = 0;
+    int n_items = 0, ktot = 0;
+};
+
+LdmLayout ldm_layout(int64_t n_var, int32_t n_sel) {
+    LdmLayout L;
+    L.ktot = (int)(((n_sel + 31) / 32 * 32 + 127) / 128 * 128);
+    L.n_items = (int)((n_var + LdmCfg::ROWS - 1) / LdmCfg::ROWS);
+    auto up = [](size_t x, size_t a) { return (x + a - 1) / a * a; };
+    size_t off = 256;
+    L.jmax = off;
+    off = up(off + (size_t)n_var * 4, 256);
+    L.items = off;
+    off = up(off + (size_t)L.n_items * 8, 1024);
+    L.planes = off;
+    off = up(off + (size_t)n_var * 2 * L.ktot, 256);
+    L.psite = off;
+    off = up(off + (size_t)n_var * 8, 256);
+    L.total = off;
+    return L;
+}
+
+template <int EST>
+cudaError_t launch_ldm(const CUtensorMap& mA, const CUtensorMap& mB, const TcArgs& a, const LdmArgs& m, int n_items,
+                       cudaStream_t s) {
+    using C = LdmCfg;
+    size_t smem = 1024 + (size_t)C::STAGES * C::STAGE_BYTES + (size_t)kEpi * 16 * kLdmStride * sizeof(double);
+    if (smem < kMinSmem) smem = kMinSmem;
+    cudaError_t e = cudaFuncSetAttribute(k_ld_matrix<EST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = n_items < sms ? n_items : sms;
+    k_ld_matrix<EST><<<grid, 128 + 32 * kEpi, smem, s>>>(mA, mB, a, m);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t ld_matrix_workspace(int64_t n_var, int32_t n_sel) { return ldm_layout(n_var, n_sel).total; }
+
+// Enqueues the all-pairs LD of the n_sel selected rows of X (see ldk_ld_matrix).
+cudaError_t launch_ld_matrix(const int8_t* X, int64_t ld_x, int64_t n_var, const int32_t* rows, int32_t n_sel,
+                             int estimator, double* out, int64_t ld_out, double* sums, unsigned char* ws,
+                             unsigned* status, cudaStream_t s) {
+    const LdmLayout L = ldm_layout(n_var, n_sel);
+    cudaError_t e;
+    int32_t* jmax = reinterpret_cast<int32_t*>(ws + L.jmax);
+    int32_t* items = reinterpret_cast<int32_t*>(ws + L.items);
+    uint8_t* planes = ws + L.planes;
+    double* psite = reinterpret_cast<double*>(ws + L.psite);
+    if (sums && (e = cudaMemsetAsync(sums, 0, 2 * sizeof(double), s)) != cudaSuccess) return e;
+    if (out && n_var > 0) {
+        k_fill_diag<<<(unsigned)((n_var + 255) / 256), 256, 0, s>>>(out, ld_out, n_var, estimator == 2 ? std::nan("") : 0.0);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (n_var < 2) return cudaSuccess;
+    // every SNP's partner range is the rest of the set
+    k_fill_int<<<(unsigned)((n_var + 255) / 256), 256, 0, s>>>(jmax, n_var, (int32_t)n_var);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    std::vector<int32_t> it;
+    it.reserve((size_t)L.n_items * 2);
+    for (int64_t r0 = 0; r0 < n_var; r0 += LdmCfg::ROWS) {  // most partners first
+        it.push_back((int32_t)r0);
+        it.push_back((int32_t)std::min<int64_t>(r0 + LdmCfg::ROWS, n_var));
+    }
+    if ((e = cudaMemcpyAsync(items, it.data(), it.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s)) != cudaSuccess)
+        return e;
+    if (estimator == 0) {
+        k_site_freq<<<(unsigned)((n_var + 255) / 256), 256, 0, s>>>(X, ld_x, n_var, rows, n_sel, psite);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    // the indicator planes of the selected rows, as for a one-population parse
+    ldk_parse_t d{};
+    d.X = X;
+    d.ld_x = ld_x;
+    d.n_var = n_var;
+    d.pop_rows = rows;
+    d.n_pops = 1;
+    d.pop_offsets[0] = 0;
+    for (int p = 1; p <= LDK_MAX_POPS; ++p) d.pop_offsets[p] = n_sel;
+    ParseShape sh{};
+    sh.P = 1;
+    sh.genotypes = 0;
+    sh.planes = 2;
+    sh.ktot = L.ktot;
+    for (int p = 0; p <= LDK_MAX_POPS; ++p) sh.kofs[p] = p == 0 ? 0 : (n_sel + 31) / 32 * 32;
+    sh.max_n = n_sel;
+    Scratch w{};
+    w.status = status;
+    w.hv = planes;
+    if ((e = launch_prep_planes(&d, w, sh, s)) != cudaSuccess) return e;
+    CUtensorMap mA, mB;
+    if (!make_map(&mA, planes, n_var, L.ktot, 2, 2, LdmCfg::ROWS) ||
+        !make_map(&mB, planes, n_var, L.ktot, 2, 2, LdmCfg::NJ))
+        return cudaErrorInvalidValue;
+    TcArgs a{};
+    a.jmax = jmax;
+    a.items = items;
+    a.n_items = L.n_items;
+    a.item_counter = reinterpret_cast<int*>(ws + 128);
+    a.nkc = L.ktot / kKChunk;
+    for (int p = 0; p <= LDK_MAX_POPS; ++p) a.kofs[p] = sh.kofs[p];
+    a.status = status;
+    LdmArgs m{psite, out, ld_out, sums};
+    switch (estimator) {
+        case 0: return launch_ldm<0>(mA, mB, a, m, L.n_items, s);
+        case 1: return launch_ldm<1>(mA, mB, a, m, L.n_items, s);
+        default: return launch_ldm<2>(mA, mB, a, m, L.n_items, s);
+    }
+}
+
+}  // namespace ldk

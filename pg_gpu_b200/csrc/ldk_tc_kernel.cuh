@@ -234,6 +234,127 @@ struct TcArgs {
     unsigned* status;
 };
 
+// Shared-memory state of the persistent pipeline (one CTA).
+struct Pipe {
+    unsigned char* stages;
+    uint64_t* full_bar;
+    uint64_t* empty_bar;
+    uint64_t* tfull;
+    uint64_t* tempty;
+    uint64_t* ifull;
+    uint64_t* iempty;
+    volatile int* ring;
+    volatile int* abort_s;
+};
+
+// Warp 0: claims row blocks from the global counter, publishes them through the ring and
+// issues the TMA loads of every partner tile's K chunks.
+template <class C>
+LDK_DEV void run_producer(const Pipe& S, const CUtensorMap* tmA, const CUtensorMap* tmB, const TcArgs& a,
+                          int lane) {
+    unsigned char* stages = S.stages;
+    uint64_t* full_bar = S.full_bar;
+    uint64_t* empty_bar = S.empty_bar;
+    uint64_t* ifull = S.ifull;
+    uint64_t* iempty = S.iempty;
+    volatile int* ring = S.ring;
+    volatile int* abort_s = S.abort_s;
+    if (lane == 0) {
+        uint32_t it = 0;
+        bool ok = true;
+        for (uint32_t k = 0; ok; ++k) {
+            // claim the next row block and publish it to the MMA issuer and the epilogue
+            const int sl = k % kRing;
+            if (!mbar_wait(&iempty[sl], ((k / kRing) & 1u) ^ 1u, abort_s, a.status)) { ok = false; break; }
+            int item = atomicAdd(a.item_counter, 1);
+            if (item >= a.n_items) item = -1;
+            ring[sl] = item;
+            mbar_arrive(&ifull[sl]);
+            if (item < 0) break;
+            const int row0 = a.items[2 * item], row1 = a.items[2 * item + 1];
+            const int jend = a.jmax[row1 - 1];
+            const int n_jt = jend > row0 + 1 ? (jend - row0 + C::NJ - 1) / C::NJ : 0;
+            for (int t = 0; t < n_jt && ok; ++t) {
+                const int j0 = row0 + t * C::NJ;
+                for (int c = 0; c < a.nkc; ++c, ++it) {
+                    const int s = it % C::STAGES;
+                    const uint32_t ph = (it / C::STAGES) & 1u;
+                    if (!mbar_wait(&empty_bar[s], ph ^ 1u, abort_s, a.status)) { ok = false; break; }
+                    unsigned char* dst = stages + s * C::STAGE_BYTES;
+                    mbar_expect_tx(&full_bar[s], C::STAGE_BYTES);
+#pragma unroll
+                    for (int x = 0; x < C::REGIONS; ++x)
+                        tma_load_3d(dst + x * C::A_BOX, tmA, &full_bar[s], c * kKChunk, x, row0);
+                    tma_load_3d(dst + C::A_BYTES, tmB, &full_bar[s], c * kKChunk, 0, j0);
+                }
+            }
+        }
+        if (!ok) spin_ns(2000000);  // let copies already issued land before teardown
+    }
+    __syncwarp();
+}
+
+// Warp 1: one thread issues the MMAs of every tile into the double-buffered accumulators.
+template <class C, int P>
+LDK_DEV void run_mma(const Pipe& S, uint32_t tmem, const TcArgs& a, int lane) {
+    unsigned char* stages = S.stages;
+    uint64_t* full_bar = S.full_bar;
+    uint64_t* empty_bar = S.empty_bar;
+    uint64_t* tfull = S.tfull;
+    uint64_t* tempty = S.tempty;
+    uint64_t* ifull = S.ifull;
+    uint64_t* iempty = S.iempty;
+    volatile int* ring = S.ring;
+    volatile int* abort_s = S.abort_s;
+    if (lane == 0) {
+        constexpr uint32_t idesc = idesc_u8<C::N>();
+        uint32_t it = 0, tcount = 0;
+        bool ok = true;
+        for (uint32_t k = 0; ok; ++k) {
+            const int sl = k % kRing;
+            if (!mbar_wait(&ifull[sl], (k / kRing) & 1u, abort_s, a.status)) { ok = false; break; }
+            const int item = ring[sl];
+            mbar_arrive(&iempty[sl]);
+            if (item < 0) break;
+            const int row0 = a.items[2 * item], row1 = a.items[2 * item + 1];
+            const int jend = a.jmax[row1 - 1];
+            const int n_jt = jend > row0 + 1 ? (jend - row0 + C::NJ - 1) / C::NJ : 0;
+            for (int t = 0; t < n_jt && ok; ++t, ++tcount) {
+                const uint32_t buf = tcount % C::NBUF, tph = (tcount / C::NBUF) & 1u;
+                if (!mbar_wait(&tempty[buf], tph ^ 1u, abort_s, a.status)) { ok = false; break; }
+                tc_fence_after();
+                for (int c = 0; c < a.nkc; ++c, ++it) {
+                    const int s = it % C::STAGES;
+                    const uint32_t ph = (it / C::STAGES) & 1u;
+                    if (!mbar_wait(&full_bar[s], ph, abort_s, a.status)) { ok = false; break; }
+                    tc_fence_after();
+                    const uint32_t a_addr = su32(stages + s * C::STAGE_BYTES);
+                    const uint32_t b_addr = a_addr + C::A_BYTES;
+#pragma unroll
+                    for (int ks = 0; ks < kKChunk / 32; ++ks) {
+                        const int kbyte = c * kKChunk + ks * 32;
+                        int p = 0;
+#pragma unroll
+                        for (int q = 1; q < P; ++q) p += (kbyte >= a.kofs[q]) ? 1 : 0;
+                        const uint32_t first = (kbyte == a.kofs[p]) ? 1u : 0u;
+#pragma unroll
+                        for (int x = 0; x < C::REGIONS; ++x) {
+                            const uint32_t d = tmem + buf * C::COLS + (p * C::REGIONS + x) * C::N;
+                            mma_u8(d, sw128_desc(a_addr + x * C::A_BOX + ks * 32), sw128_desc(b_addr + ks * 32),
+                                   idesc, first ^ 1u);
+                        }
+                    }
+                    mma_commit(&empty_bar[s]);
+                }
+                if (!ok) break;
+                mma_commit(&tfull[buf]);
+            }
+        }
+        if (!ok) spin_ns(2000000);
+    }
+    __syncwarp();
+}
+
 template <int P, typename T, bool PRIV, bool GENO, int V>
 __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
     k_parse_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcArgs a) {
@@ -286,91 +407,9 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_base_s;
-    if (warp == 0) {
-        // ------------------------------------------------------------- TMA producer
-        if (lane == 0) {
-            uint32_t it = 0;
-            bool ok = true;
-            for (uint32_t k = 0; ok; ++k) {
-                // claim the next row block and publish it to the MMA issuer and the epilogue
-                const int sl = k % kRing;
-                if (!mbar_wait(&iempty[sl], ((k / kRing) & 1u) ^ 1u, &abort_s, a.status)) { ok = false; break; }
-                int item = atomicAdd(a.item_counter, 1);
-                if (item >= a.n_items) item = -1;
-                ring[sl] = item;
-                mbar_arrive(&ifull[sl]);
-                if (item < 0) break;
-                const int row0 = a.items[2 * item], row1 = a.items[2 * item + 1];
-                const int jend = a.jmax[row1 - 1];
-                const int n_jt = jend > row0 + 1 ? (jend - row0 + C::NJ - 1) / C::NJ : 0;
-                for (int t = 0; t < n_jt && ok; ++t) {
-                    const int j0 = row0 + t * C::NJ;
-                    for (int c = 0; c < a.nkc; ++c, ++it) {
-                        const int s = it % C::STAGES;
-                        const uint32_t ph = (it / C::STAGES) & 1u;
-                        if (!mbar_wait(&empty_bar[s], ph ^ 1u, &abort_s, a.status)) { ok = false; break; }
-                        unsigned char* dst = stages + s * C::STAGE_BYTES;
-                        mbar_expect_tx(&full_bar[s], C::STAGE_BYTES);
-#pragma unroll
-                        for (int x = 0; x < C::REGIONS; ++x)
-                            tma_load_3d(dst + x * C::A_BOX, &tmA, &full_bar[s], c * kKChunk, x, row0);
-                        tma_load_3d(dst + C::A_BYTES, &tmB, &full_bar[s], c * kKChunk, 0, j0);
-                    }
-                }
-            }
-            if (!ok) spin_ns(2000000);  // let copies already issued land before teardown
-        }
-        __syncwarp();
-    } else if (warp == 1) {
-        // ------------------------------------------------------------- MMA issuer
-        if (lane == 0) {
-            constexpr uint32_t idesc = idesc_u8<C::N>();
-            uint32_t it = 0, tcount = 0;
-            bool ok = true;
-            for (uint32_t k = 0; ok; ++k) {
-                const int sl = k % kRing;
-                if (!mbar_wait(&ifull[sl], (k / kRing) & 1u, &abort_s, a.status)) { ok = false; break; }
-                const int item = ring[sl];
-                mbar_arrive(&iempty[sl]);
-                if (item < 0) break;
-                const int row0 = a.items[2 * item], row1 = a.items[2 * item + 1];
-                const int jend = a.jmax[row1 - 1];
-                const int n_jt = jend > row0 + 1 ? (jend - row0 + C::NJ - 1) / C::NJ : 0;
-                for (int t = 0; t < n_jt && ok; ++t, ++tcount) {
-                    const uint32_t buf = tcount % C::NBUF, tph = (tcount / C::NBUF) & 1u;
-                    if (!mbar_wait(&tempty[buf], tph ^ 1u, &abort_s, a.status)) { ok = false; break; }
-                    tc_fence_after();
-                    for (int c = 0; c < a.nkc; ++c, ++it) {
-                        const int s = it % C::STAGES;
-                        const uint32_t ph = (it / C::STAGES) & 1u;
-                        if (!mbar_wait(&full_bar[s], ph, &abort_s, a.status)) { ok = false; break; }
-                        tc_fence_after();
-                        const uint32_t a_addr = su32(stages + s * C::STAGE_BYTES);
-                        const uint32_t b_addr = a_addr + C::A_BYTES;
-#pragma unroll
-                        for (int ks = 0; ks < kKChunk / 32; ++ks) {
-                            const int kbyte = c * kKChunk + ks * 32;
-                            int p = 0;
-#pragma unroll
-                            for (int q = 1; q < P; ++q) p += (kbyte >= a.kofs[q]) ? 1 : 0;
-                            const uint32_t first = (kbyte == a.kofs[p]) ? 1u : 0u;
-#pragma unroll
-                            for (int x = 0; x < C::REGIONS; ++x) {
-                                const uint32_t d = tmem + buf * C::COLS + (p * C::REGIONS + x) * C::N;
-                                mma_u8(d, sw128_desc(a_addr + x * C::A_BOX + ks * 32), sw128_desc(b_addr + ks * 32),
-                                       idesc, first ^ 1u);
-                            }
-                        }
-                        mma_commit(&empty_bar[s]);
-                    }
-                    if (!ok) break;
-                    mma_commit(&tfull[buf]);
-                }
-            }
-            if (!ok) spin_ns(2000000);
-        }
-        __syncwarp();
-    }
+    const Pipe pipe{stages, full_bar, empty_bar, tfull, tempty, ifull, iempty, ring, &abort_s};
+    if (warp == 0) run_producer<C>(pipe, &tmA, &tmB, a, lane);
+    else if (warp == 1) run_mma<C, P>(pipe, tmem, a, lane);
     if (warp >= 4) {
         // ------------------------------------------------------------- epilogue
         const int e = warp - 4;

@@ -166,6 +166,26 @@ class HaplotypeMatrix:
             out[key] = tuple(vals) if as_tuple else OrderedDict(zip(names, vals))
         return out
 
+    def pairwise_r2(self, estimator="r2"):
+        """(n_variants, n_variants) float64 pairwise r^2 on the GPU
+        (haplotype_matrix.py:1138-1175); ``estimator='sigma_d2'`` gives the unbiased
+        sigma_D^2 matrix instead.  Rogers-Huff dosage r^2 is not provided here."""
+        from .ld_matrix import ld_matrix
+        if estimator not in ("r2", "sigma_d2"):
+            raise ValueError(f"Unknown estimator: {estimator!r} (expected 'r2' or 'sigma_d2')")
+        self.transfer_to_gpu()
+        return ld_matrix(self.haplotypes, estimator=estimator)[0]
+
+    def windowed_r_squared(self, bp_bins, percentile=50, pop=None, estimator="r2"):
+        """Percentiles of r^2 per genomic distance bin and pair counts
+        (haplotype_matrix.py:1235-1317), over the rows of ``pop`` (default: all)."""
+        from .ld_matrix import windowed_r_squared
+        if estimator != "r2":
+            raise NotImplementedError("only the 'r2' estimator is provided")
+        self.transfer_to_gpu()
+        rows = None if pop is None else self.sample_sets[pop]
+        return windowed_r_squared(self.haplotypes, self._np(self.positions), bp_bins, percentile, rows=rows)
+
     def compute_ld_statistics_gpu_single_pop(self, bp_bins, raw=False, ac_filter=True, chunk_size="auto",
                                              method="tc"):
         """{(lo, hi): (DD, Dz, pi2)} over all haplotypes, sums if ``raw`` else means

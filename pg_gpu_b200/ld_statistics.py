@@ -131,3 +131,39 @@ def r_squared(counts, n_valid=None):
 def d_prime(counts, n_valid=None):
     """Lewontin's D' per pair (ld_statistics.py:220-246)."""
     return _r_family(2, counts, n_valid)
+
+
+def zns(r2_matrix_or_matrix, missing_data="include", estimator="auto"):
+    """Kelly's ZnS (ld_statistics.py:679-718): a HaplotypeMatrix goes through the
+    all-pairs kernel (no matrix is materialised); a precomputed square r^2 matrix gives
+    (sum - trace) / (m (m - 1))."""
+    from .haplotype_matrix import HaplotypeMatrix
+    from . import ld_matrix
+    if isinstance(r2_matrix_or_matrix, HaplotypeMatrix):
+        r2_matrix_or_matrix.transfer_to_gpu()
+        return ld_matrix.zns(r2_matrix_or_matrix.haplotypes, missing_data, estimator)
+    if estimator == "sigma_d2":
+        raise ValueError("estimator='sigma_d2' requires a HaplotypeMatrix, not a pre-computed r^2 array")
+    if hasattr(r2_matrix_or_matrix, "genotypes"):
+        raise NotImplementedError("diploid r^2 matrices are not provided; pass a HaplotypeMatrix or an r^2 array")
+    torch = _lib.require_cuda()
+    M = torch.as_tensor(r2_matrix_or_matrix, dtype=torch.float64, device="cuda")
+    m = M.shape[0]
+    if m < 2:
+        return 0.0
+    return float(((M.sum() - torch.trace(M)) / (m * (m - 1))).item())
+
+
+def omega(r2_matrix_or_matrix, missing_data="include", estimator="auto"):
+    """Kim & Nielsen's Omega (ld_statistics.py:761-862) of a HaplotypeMatrix (all-pairs
+    kernel on its segregating sites) or of a precomputed r^2 matrix."""
+    from .haplotype_matrix import HaplotypeMatrix
+    from . import ld_matrix
+    if isinstance(r2_matrix_or_matrix, HaplotypeMatrix):
+        r2_matrix_or_matrix.transfer_to_gpu()
+        return ld_matrix.omega(r2_matrix_or_matrix.haplotypes, missing_data, estimator)
+    if estimator == "sigma_d2":
+        raise ValueError("estimator='sigma_d2' requires a HaplotypeMatrix")
+    if hasattr(r2_matrix_or_matrix, "genotypes"):
+        raise NotImplementedError("diploid r^2 matrices are not provided; pass a HaplotypeMatrix or an r^2 array")
+    return ld_matrix.omega_from_matrix(r2_matrix_or_matrix)
