@@ -4,10 +4,10 @@
 //
 // The Gram counts come from the same TMA + tcgen05 pipeline as the binned parse (64-SNP
 // row blocks against 128-SNP partner tiles, no distance cutoff, so every partner j > i of
-// the set).  Each epilogue warp evaluates its 16 rows x 128 partners of a tile into a
-// padded shared-memory tile and then writes the tile's rows (upper triangle, 1 KB runs)
-// and columns (lower triangle, 128-byte runs) with coalesced stores: the kernel is bound
-// by the n^2 x 8 bytes it writes.
+// the set).  Four epilogue warps share each TMEM lane quarter (16 SNPs), one per quarter
+// of the partner tile; each evaluates its 16 rows x 32 partners into a padded
+// shared-memory tile and then writes the tile's rows (upper triangle, 256-byte runs) and
+// columns (lower triangle, 128-byte runs) with coalesced stores.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -19,7 +19,10 @@ namespace ldk {
 namespace {
 
 using LdmCfg = Cfg<1, false, 0>;
-constexpr int kLdmStride = LdmCfg::NJ + 1;  // staging row stride (doubles): rows hit distinct banks
+constexpr int kLdmEpi = 16;                    // epilogue warps: four per TMEM lane quarter
+constexpr int kLdmParts = kLdmEpi / 4;         // partner ranges a tile is split into
+constexpr int kLdmHalf = LdmCfg::NJ / kLdmParts;  // partners per epilogue warp and tile
+constexpr int kLdmStride = kLdmHalf + 1;       // staging row stride (doubles): rows hit distinct banks
 
 struct LdmArgs {
     const double* psite;  // per SNP: derived allele frequency over the site's valid haplotypes
@@ -54,7 +57,7 @@ __global__ void k_site_freq(const int8_t* __restrict__ X, int64_t ld, int64_t n_
 }
 
 template <int EST>
-__global__ void __launch_bounds__(128 + 32 * kEpi, 1)
+__global__ void __launch_bounds__(128 + 32 * kLdmEpi, 1)
     k_ld_matrix(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcArgs a,
                 const LdmArgs m) {
     using C = LdmCfg;
@@ -62,7 +65,7 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
     extern __shared__ unsigned char smem_raw[];
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     unsigned char* stages = base;
-    double* stile = reinterpret_cast<double*>(base + C::STAGES * C::STAGE_BYTES);  // [kEpi][16][SP]
+    double* stile = reinterpret_cast<double*>(base + C::STAGES * C::STAGE_BYTES);  // [kLdmEpi][16][SP]
 
     __shared__ __align__(8) uint64_t full_bar[C::STAGES], empty_bar[C::STAGES], tfull[C::NBUF], tempty[C::NBUF];
     __shared__ __align__(8) uint64_t ifull[kRing], iempty[kRing];
@@ -78,11 +81,11 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
         }
         for (int b = 0; b < C::NBUF; ++b) {
             mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], kEpi);
+            mbar_init(&tempty[b], kLdmEpi);
         }
         for (int b = 0; b < kRing; ++b) {
             mbar_init(&ifull[b], 1);
-            mbar_init(&iempty[b], 1 + kEpi);
+            mbar_init(&iempty[b], 1 + kLdmEpi);
         }
         abort_s = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -99,8 +102,9 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
     if (warp == 0) run_producer<C>(pipe, &tmA, &tmB, a, lane);
     else if (warp == 1) run_mma<C, 1>(pipe, tmem, a, lane);
     if (warp >= 4) {
-        // lanes 2r, 2r+1 share SNP r (16 per warp) and split its partners by parity
-        const int e = warp - 4, quarter = warp & 3;
+        // lanes 2r, 2r+1 share SNP r (16 per warp) and split its partners by parity; the
+        // warp takes part `half` (of kLdmParts) of every partner tile
+        const int e = warp - 4, quarter = warp & 3, half = e >> 2;
         const int rr = lane >> 1, role = lane & 1;
         const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
         double* st = stile + e * 16 * SP;
@@ -116,7 +120,7 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
                 }
             }
             item = __shfl_sync(0xffffffffu, item, 0);
-            if (epi_bar_or<kEpi>(abort_s != 0 || item < 0)) break;
+            if (epi_bar_or<kLdmEpi>(abort_s != 0 || item < 0)) break;
             const int row0 = a.items[2 * item], row1 = a.items[2 * item + 1];
             const int jend = a.jmax[row1 - 1];
             const int n_jt = jend > row0 + 1 ? (jend - row0 + NJ - 1) / NJ : 0;
@@ -128,26 +132,28 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
             for (int t = 0; t < n_jt; ++t, ++tcount) {
                 const uint32_t buf = tcount % C::NBUF, tph = (tcount / C::NBUF) & 1u;
                 const int j0 = row0 + t * NJ;
-                double preg[NJ / 32];
+                double preg[(kLdmHalf + 31) / 32];
 #pragma unroll
-                for (int kk = 0; kk < NJ / 32; ++kk) {
-                    const int j = j0 + 32 * kk + lane;
+                for (int kk = 0; kk < (kLdmHalf + 31) / 32; ++kk) {
+                    const int j = j0 + half * kLdmHalf + 32 * kk + lane;
                     preg[kk] = (EST == 0 && j < jend) ? m.psite[j] : 0.0;
                 }
                 if (!mbar_wait(&tfull[buf], tph, &abort_s, a.status)) { ok = false; break; }
                 tc_fence_after();
 #pragma unroll 1
-                for (int q = 0; q < NJ / 2; ++q) {
+                for (int qh = 0; qh < kLdmHalf / 2; ++qh) {
+                    const int q = half * (kLdmHalf / 2) + qh;
                     uint32_t v[1][4];
                     tmem_ld4(tmem + lane_base + buf * C::COLS + q * 4, v[0]);
-                    const int jj = 2 * q + role;
+                    const int jl = 2 * qh + role;  // partner within this warp's half tile
+                    const int jj = half * kLdmHalf + jl;
                     double psrc = preg[0];
 #pragma unroll
-                    for (int kk = 1; kk < NJ / 32; ++kk)
-                        if ((jj >> 5) == kk) psrc = preg[kk];
-                    const double pj = __shfl_sync(0xffffffffu, psrc, jj & 31);
+                    for (int kk = 1; kk < (kLdmHalf + 31) / 32; ++kk)
+                        if ((jl >> 5) == kk) psrc = preg[kk];
+                    const double pj = __shfl_sync(0xffffffffu, psrc, jl & 31);
                     tmem_wait4<1>(v);
-                    if (q == NJ / 2 - 1) {
+                    if (qh == kLdmHalf / 2 - 1) {
                         tc_fence_before();
                         __syncwarp();
                         if (lane == 0) mbar_arrive(&tempty[buf]);
@@ -167,10 +173,10 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
                         const double c1 = hh, c2 = hv - hh, c3 = vh - hh, c4 = vv - hv - vh + hh, n = vv;
                         if constexpr (EST == 0) {
                             // haplotype_matrix.py:1122-1128, 1171-1175
-                            const double pab = n > 0.0 ? c1 / n : 0.0;
+                            const double pab = n > 0.0 ? c1 * recip_newton(n) : 0.0;
                             const double D = pab - pi * pj;
                             const double den = (pi * (1.0 - pi)) * (pj * (1.0 - pj));
-                            val = den > 0.0 ? D * D / den : 0.0;
+                            val = den > 0.0 ? (D * D) * recip_newton(den) : 0.0;
                             zsum += val;
                             zcnt += 1.0;
                         } else if constexpr (EST == 1) {
@@ -181,7 +187,7 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
                             const double pi2 = s12 * s13 * s24 * s34 - c1 * c4 * (-1.0 + c1 + 3.0 * c2 + 3.0 * c3 + c4) -
                                                c2 * c3 * (-1.0 + 3.0 * c1 + c2 + c3 + 3.0 * c4);
                             const bool nok = n >= 4.0;
-                            val = (nok && pi2 != 0.0) ? dd / pi2 : 0.0;
+                            val = (nok && pi2 != 0.0) ? dd * recip_newton(pi2) : 0.0;
                             zsum += val;
                             zcnt += nok ? 1.0 : 0.0;
                         } else {
@@ -189,7 +195,7 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
                             const double D = c1 * c4 - c2 * c3;
                             const double den = (c1 + c2) * (c3 + c4) * ((c1 + c3) * (c2 + c4));
                             if (den > 0.0) {
-                                val = D * D / den;
+                                val = (D * D) * recip_newton(den);
                                 zsum += val;
                                 zcnt += 1.0;
                             } else {
@@ -197,17 +203,17 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
                             }
                         }
                     }
-                    st[rr * SP + jj] = val;
+                    st[rr * SP + jl] = val;
                 }
                 __syncwarp();
                 if (m.out) {
-                    const int gi0 = row0 + quarter * 16;
-                    for (int idx = lane; idx < 16 * NJ; idx += 32) {  // rows: upper triangle
-                        const int r = idx / NJ, c = idx % NJ, gi = gi0 + r, gj = j0 + c;
+                    const int gi0 = row0 + quarter * 16, gj0 = j0 + half * kLdmHalf;
+                    for (int idx = lane; idx < 16 * kLdmHalf; idx += 32) {  // rows: upper triangle
+                        const int r = idx / kLdmHalf, c = idx % kLdmHalf, gi = gi0 + r, gj = gj0 + c;
                         if (gi < row1 && gj > gi && gj < jend) m.out[(int64_t)gi * m.ld_out + gj] = st[r * SP + c];
                     }
-                    for (int idx = lane; idx < 16 * NJ; idx += 32) {  // columns: lower triangle
-                        const int r = idx % 16, c = idx / 16, gi = gi0 + r, gj = j0 + c;
+                    for (int idx = lane; idx < 16 * kLdmHalf; idx += 32) {  // columns: lower triangle
+                        const int r = idx % 16, c = idx / 16, gi = gi0 + r, gj = gj0 + c;
                         if (gi < row1 && gj > gi && gj < jend) m.out[(int64_t)gj * m.ld_out + gi] = st[r * SP + c];
                     }
                 }
@@ -262,7 +268,7 @@ template <int EST>
 cudaError_t launch_ldm(const CUtensorMap& mA, const CUtensorMap& mB, const TcArgs& a, const LdmArgs& m, int n_items,
                        cudaStream_t s) {
     using C = LdmCfg;
-    size_t smem = 1024 + (size_t)C::STAGES * C::STAGE_BYTES + (size_t)kEpi * 16 * kLdmStride * sizeof(double);
+    size_t smem = 1024 + (size_t)C::STAGES * C::STAGE_BYTES + (size_t)kLdmEpi * 16 * kLdmStride * sizeof(double);
     if (smem < kMinSmem) smem = kMinSmem;
     cudaError_t e = cudaFuncSetAttribute(k_ld_matrix<EST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -270,7 +276,7 @@ cudaError_t launch_ldm(const CUtensorMap& mA, const CUtensorMap& mB, const TcArg
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int grid = n_items < sms ? n_items : sms;
-    k_ld_matrix<EST><<<grid, 128 + 32 * kEpi, smem, s>>>(mA, mB, a, m);
+    k_ld_matrix<EST><<<grid, 128 + 32 * kLdmEpi, smem, s>>>(mA, mB, a, m);
     return cudaGetLastError();
 }
 
