@@ -209,9 +209,17 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="call ldk_parse per step instead of a graph replay")
     ap.add_argument("--no-autotune", action="store_true", help="default tile width, no tuning")
+    ap.add_argument("--all-pairs", action="store_true",
+                    help="time the all-pairs LD kernel (ldk_ld_matrix) instead of the binned parse")
+    ap.add_argument("--snps", type=int, default=24576, help="--all-pairs: SNPs in the set")
+    ap.add_argument("--haplotypes", type=int, default=200, help="--all-pairs: haplotypes")
+    ap.add_argument("--estimator", choices=["r2", "sigma_d2", "r2_counts"], default="r2")
+    ap.add_argument("--reduce-only", action="store_true", help="--all-pairs: ZnS sums only, no matrix")
     args = ap.parse_args()
 
     ws, rank, local = dist_env()
+    if args.all_pairs:
+        return run_all_pairs(args)
     if args.impl == "reference":
         return run_reference(args, ws, rank)
 
@@ -458,6 +466,65 @@ def main():
         print(json.dumps(line), flush=True)
     if ws > 1:
         dist.destroy_process_group()
+
+
+def run_all_pairs(args):
+    """All-pairs LD of one SNP set (pairwise r^2 / sigma_D^2 / count r^2 for every pair,
+    the matrix written to HBM unless --reduce-only): one JSON line, roofline against HBM
+    (matrix bytes written) or, reduce-only, against the INT8 tensor peak."""
+    import torch
+    from pg_gpu_b200 import _lib, ld_matrix, synth
+    lib = _lib.load()
+    rng = np.random.default_rng(6)
+    m, n = args.snps, args.haplotypes
+    hap, _pos = synth.haplotype_region(rng, [n], m, m * 100, 0.01)
+    X = torch.as_tensor(np.ascontiguousarray(hap), device="cuda")
+    R = torch.arange(n, dtype=torch.int32, device="cuda")
+    M = None if args.reduce_only else torch.empty((m, m), dtype=torch.float64, device="cuda")
+    S = torch.zeros(2, dtype=torch.float64, device="cuda")
+    wsb = torch.empty(int(lib.ldk_ld_matrix_workspace_size(m, n)), dtype=torch.uint8, device="cuda")
+    est = ld_matrix.ESTIMATORS[args.estimator]
+
+    def step():
+        _lib.check(lib.ldk_ld_matrix(_lib.ptr(X), m, m, _lib.ptr(R), n, est, _lib.ptr(M), m, _lib.ptr(S),
+                                     _lib.ptr(wsb), wsb.numel(), _lib.stream_handle()))
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    pairs = m * (m - 1) // 2
+    pk_d, pk_kind = peaks()
+    probe_i8, _ = _lib.probe_peaks()
+    if M is not None:
+        bytes_ = m * m * 8
+        roof = {"bound": "hbm", "achieved": bytes_ / (ms / 1e3) / 1e9, "peak": pk_d["hbm_gbs"], "unit": "GB/s",
+                "peak_source": f"{pk_kind} copy bandwidth", "algorithmic_bytes": bytes_}
+    else:
+        ops = 8 * n * pairs
+        roof = {"bound": "tensor", "achieved": ops / (ms / 1e3) / 1e12, "peak": probe_i8 / 1e12,
+                "unit": "TOP/s (INT8, MAC=2)", "peak_source": "measured in this run: ldk_probe_peaks"}
+    roof["frac"] = roof["achieved"] / roof["peak"]
+    roof["traffic"] = None
+    print(json.dumps({
+        "metric": "all-pairs LD SNP-pairs/s", "value": pairs / (ms / 1e3), "unit": "SNP-pairs/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8 counts / s32 accumulate / f64 values",
+        "data": "synthetic (seeded founder mosaics, 1% missing)",
+        "config": {"workload": f"all-pairs {args.estimator}, {m} SNPs x {n} haplotypes",
+                   "matrix": M is not None, "pairs": pairs, "l2": "matrix larger than L2" if M is not None else
+                   "reduction only"},
+        "roofline": roof, "gpu_launches": int(args.steps * ((M is not None) + (est == 0) + 3)),
+        "clocks": clk.summary()}),
+        flush=True)
 
 
 def parser_ktot(w):
