@@ -967,3 +967,93 @@ def windowed_r2(hap, positions, bp_bins, percentile=50):
         if len(sel):
             res[k] = np.percentile(sel, pct)
     return (res[:, 0] if res.shape[1] == 1 else res), cnt
+
+
+def _geno_cells_all_pairs(geno):
+    """Nine-cell counts n_ab (a = g_i, b = g_j, both valid) for all column pairs, as the
+    list [n00, n01, ..., n22] of (m, m) arrays (ld_pipeline.py:183-263 column order)."""
+    g = np.asarray(geno)
+    ind = [(g == a).astype(np.float64) for a in range(3)]
+    return [ind[a].T @ ind[b] for a in range(3) for b in range(3)]
+
+
+def rogers_huff_r(geno):
+    """Condensed upper-triangle Rogers-Huff r of dosages without missing calls
+    (ld_statistics.py:392-524): cov = g_i . g_j - n mu_i mu_j, r = cov / sqrt(ssd_i ssd_j),
+    NaN where either site is constant."""
+    g = np.asarray(geno, dtype=np.float64)
+    n = g.shape[0]
+    mu = g.mean(axis=0)
+    ssd = ((g - mu) ** 2).sum(axis=0)
+    cov = g.T @ g - n * np.outer(mu, mu)
+    den = np.sqrt(np.outer(ssd, ssd))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        r = np.where(den > 0, cov / np.where(den > 0, den, 1), np.nan)
+    iu = np.triu_indices(g.shape[1], k=1)
+    return r[iu]
+
+
+def diploid_r2_matrix(geno):
+    """Dosage r^2 with missing calls (ld_statistics.py:973-1021): dosages centred on the
+    site's valid mean and zeroed where missing, cov = gn_i . gn_j, r^2 = cov^2 / (var_i
+    var_j), 0 where that product is 0; diagonal 0."""
+    g = np.asarray(geno)
+    v = (g >= 0).astype(np.float64)
+    gc = np.where(g >= 0, g, 0).astype(np.float64)
+    nv = v.sum(axis=0)
+    mean = np.where(nv > 0, gc.sum(axis=0) / np.where(nv > 0, nv, 1), 0.0)
+    gn = (gc - mean[None, :]) * v
+    var = (gn ** 2).sum(axis=0)
+    cov = gn.T @ gn
+    den = np.sqrt(np.outer(var, var))
+    r2 = np.where(den > 0, (cov / np.where(den > 0, den, 1)) ** 2, 0.0)
+    np.fill_diagonal(r2, 0.0)
+    return r2
+
+
+def sigma_d2_geno(geno):
+    """Condensed upper-triangle unbiased sigma_D^2 of genotype pairs (genotype_kernels.py:
+    91-170, ld_statistics_genotype.py:1518-1598): DD numerator over pi2 numerator (their
+    denominators cancel), NaN where fewer than 4 individuals or the pi2 numerator <= 0."""
+    cells = _geno_cells_all_pairs(geno)
+    iu = np.triu_indices(np.asarray(geno).shape[1], k=1)
+    c = np.stack([x[iu] for x in cells], axis=1)
+    n1, n2, n3, n4, n5, n6, n7, n8, n9 = to_moments_order(c)
+    ns = n1 + n2 + n3 + n4 + n5 + n6 + n7 + n8 + n9
+    Dg = (-(0.5 * n2 + n3 + 0.25 * n5 + 0.5 * n6) * (0.5 * n4 + 0.25 * n5 + n7 + 0.5 * n8)
+          + (n1 + 0.5 * n2 + 0.5 * n4 + 0.25 * n5) * (0.25 * n5 + 0.5 * n6 + 0.5 * n8 + n9))
+    g9 = [n1, n2, n3, n4, n5, n6, n7, n8, n9]
+    dd = (geno_dd_single_num(g9) / 16.0 + Dg * Dg) * 4.0
+    a1 = n1 + n2 + n3 + 0.5 * n4 + 0.5 * n5 + 0.5 * n6
+    a2 = n1 + 0.5 * n2 + n4 + 0.5 * n5 + n7 + 0.5 * n8
+    a3 = 0.5 * n2 + n3 + 0.5 * n5 + n6 + 0.5 * n8 + n9
+    a4 = 0.5 * n4 + 0.5 * n5 + 0.5 * n6 + n7 + n8 + n9
+    pi2 = a1 * a2 * a3 * a4 + geno_pi2_single_corr(g9) / 16.0
+    with np.errstate(divide="ignore", invalid="ignore"):
+        out = np.where((ns >= 4) & (pi2 > 0), dd / np.where(pi2 > 0, pi2, 1), np.nan)
+    return out
+
+
+def zns_diploid(geno):
+    """ZnS of a GenotypeMatrix (ld_statistics.py:679-735 via _resolve_r2_matrix, :926-972):
+    mean off-diagonal dosage r^2."""
+    r2 = diploid_r2_matrix(geno)
+    m = r2.shape[0]
+    return 0.0 if m < 2 else float((r2.sum() - np.trace(r2)) / (m * (m - 1)))
+
+
+def omega_diploid(geno):
+    """Omega of a GenotypeMatrix on its dosage r^2 matrix (ld_statistics.py:761-862)."""
+    r2 = diploid_r2_matrix(geno)
+    m = r2.shape[0]
+    if m < 5:
+        return 0.0
+    up = np.triu(r2, k=1)
+    best = 0.0
+    for l in range(3, m - 1):
+        left, cross, right = up[:l, :l].sum(), up[:l, l:].sum(), up[l:, l:].sum()
+        n_within = l * (l - 1) // 2 + (m - l) * (m - l - 1) // 2
+        n_cross = l * (m - l)
+        if n_within > 0 and n_cross > 0 and cross > 0:
+            best = max(best, ((left + right) / n_within) / (cross / n_cross))
+    return float(best)

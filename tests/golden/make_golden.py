@@ -252,6 +252,26 @@ def make_ldm_fixtures(reference):
         out[f"win{k}_pct"] = np.atleast_1d(pct).astype(np.float64)
         out[f"win{k}_res"] = np.asarray(res)
         out[f"win{k}_cnt"] = np.asarray(cnt)
+    # genotype path: Rogers-Huff r and sigma_D^2 (no missing calls), dosage r^2, ZnS and
+    # Omega of a GenotypeMatrix (with missing calls)
+    mods_g = ref_shim.import_reference_modules(
+        reference, ["ld_statistics", "genotype_matrix", "ld_statistics_genotype", "ld_pipeline", "genotype_kernels"])
+    Lg = mods_g["ld_statistics"]
+    for fn in ("sum", "max", "trace", "digitize"):
+        f = getattr(np, fn)
+        setattr(sys.modules["cupy"], fn, (lambda f: lambda *a, **k: np.asarray(f(*a, **k)).view(_A))(f))
+    GM = mods_g["genotype_matrix"].GenotypeMatrix
+    geno = (hap[0::2].clip(0) + hap[1::2].clip(0)).astype(np.int8)   # 32 diploids, no missing
+    gpos = pos.copy()
+    out["geno"] = geno
+    out["rogers_huff_r"] = np.asarray(Lg.rogers_huff_r(GM(geno.copy(), gpos.copy())))
+    out["sigma_d2_geno"] = np.asarray(mods_g["ld_statistics_genotype"].sigma_d2_geno(GM(geno.copy(), gpos.copy())))
+    geno_m = geno.copy()
+    geno_m[np.random.default_rng(78).random(geno_m.shape) < 0.04] = -1
+    out["geno_missing"] = geno_m
+    out["diploid_r2"] = np.asarray(Lg._r2_matrix_diploid(GM(geno_m.copy(), gpos.copy())))
+    out["zns_diploid"] = np.float64(Lg.zns(GM(geno_m.copy(), gpos.copy())))
+    out["omega_diploid"] = np.float64(Lg.omega(GM(geno_m.copy(), gpos.copy())))
     np.savez_compressed(os.path.join(HERE, "ref_ldm.npz"), **out)
 
 

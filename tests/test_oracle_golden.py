@@ -168,3 +168,14 @@ def test_all_pairs_ld_oracle_matches_reference(golden_dir):
         res, cnt = O.windowed_r2(hap, pos, g[f"win{k}_bins"], pct if len(pct) > 1 else pct[0])
         np.testing.assert_array_equal(cnt, g[f"win{k}_cnt"])
         np.testing.assert_allclose(res, g[f"win{k}_res"], rtol=1e-12, equal_nan=True)
+
+
+def test_all_pairs_genotype_oracle_matches_reference(golden_dir):
+    """Rogers-Huff r, sigma_D^2 of genotype pairs, dosage r^2 with missing calls, and ZnS /
+    Omega of a GenotypeMatrix, against the reference's own functions."""
+    g = np.load(os.path.join(golden_dir, "ref_ldm.npz"))
+    np.testing.assert_allclose(O.rogers_huff_r(g["geno"]), g["rogers_huff_r"], rtol=1e-12, equal_nan=True)
+    np.testing.assert_allclose(O.sigma_d2_geno(g["geno"]), g["sigma_d2_geno"], rtol=1e-12, equal_nan=True)
+    np.testing.assert_allclose(O.diploid_r2_matrix(g["geno_missing"]), g["diploid_r2"], rtol=1e-12, atol=1e-15)
+    np.testing.assert_allclose(O.zns_diploid(g["geno_missing"]), g["zns_diploid"], rtol=1e-12)
+    np.testing.assert_allclose(O.omega_diploid(g["geno_missing"]), g["omega_diploid"], rtol=1e-12)
