@@ -149,8 +149,8 @@ LDK_API int ldk_parse_enqueue(const ldk_parse_t* d, const ldk_parse_out_t* out, 
                               size_t workspace_bytes, void* stream);
 LDK_API int ldk_parse_status(const void* workspace, void* stream);
 
-/* All-pairs LD of one SNP set: for the n_sel selected rows of X (haplotypes, int8 in
- * {-1, 0, 1}) and every pair of its n_var SNPs, one of
+/* All-pairs LD of one SNP set: for the n_sel selected rows of X and every pair of its
+ * n_var SNPs, one of -- for haplotypes (X int8 in {-1, 0, 1}):
  *   LDK_LDM_R2        pg_gpu's pairwise r^2 (HaplotypeMatrix.pairwise_r2('r2'),
  *                     haplotype_matrix.py:1092-1175): D = p_AB - p_i p_j with p_AB over the
  *                     jointly valid haplotypes and p_i over the site's valid ones,
@@ -160,14 +160,30 @@ LDK_API int ldk_parse_status(const void* workspace, void* stream);
  *                     diagonal 0;
  *   LDK_LDM_R2_COUNTS r^2 from the jointly valid counts (ld_statistics.r_squared,
  *                     haplotype_kernels.py:32-42): NaN where pA qA pB qB = 0; diagonal NaN.
+ * For genotypes (X int8 in {-1, 0, 1, 2}, rows = individuals):
+ *   LDK_LDM_DIPLOID_R2    pg_gpu's dosage r^2 (ld_statistics._r2_matrix_diploid,
+ *                         ld_statistics.py:973-1021): dosages centred on the site's valid
+ *                         mean and zeroed where missing, r^2 = cov^2 / (var_i var_j), 0 where
+ *                         that product is 0; diagonal 0;
+ *   LDK_LDM_ROGERS_HUFF_R signed Rogers-Huff r (ld_statistics.py:392-524), complete data
+ *                         only: NaN where a site is constant; diagonal NaN;
+ *   LDK_LDM_SIGMA_D2_GENO the unbiased sigma_D^2 of genotype pairs (genotype_kernels.py:91-170),
+ *                         complete data only: NaN where n < 4 or the pi2 numerator <= 0;
+ *                         diagonal NaN.  A missing call with the last two sets the device
+ *                         status (LDK_ERR_DEVICE).
  * out (device, may be NULL): n_var rows of ld_out doubles, the full symmetric matrix.
  * sums (device double[2], may be NULL): the sum of the values over pairs i < j that enter
  * ZnS's mean and their count -- every pair for LDK_LDM_R2, pairs with n >= 4 for
- * LDK_LDM_SIGMA_D2 (ld_statistics.py:534-596), finite values for LDK_LDM_R2_COUNTS.
+ * LDK_LDM_SIGMA_D2 (ld_statistics.py:534-596), finite values for LDK_LDM_R2_COUNTS; every
+ * pair for LDK_LDM_DIPLOID_R2; for the other two the sum of r^2 (resp. sigma_D^2) over
+ * finite values and their count.
  * Counts come from the tensor-core Gram pipeline; values in FP64.  Synchronises `stream`. */
 #define LDK_LDM_R2 0
 #define LDK_LDM_SIGMA_D2 1
 #define LDK_LDM_R2_COUNTS 2
+#define LDK_LDM_DIPLOID_R2 3
+#define LDK_LDM_ROGERS_HUFF_R 4
+#define LDK_LDM_SIGMA_D2_GENO 5
 LDK_API size_t ldk_ld_matrix_workspace_size(int64_t n_var, int32_t n_sel);
 LDK_API int ldk_ld_matrix(const int8_t* X, int64_t ld_x, int64_t n_var, const int32_t* rows, int32_t n_sel,
                           int estimator, double* out, int64_t ld_out, double* sums, void* workspace,

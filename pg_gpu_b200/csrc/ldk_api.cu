@@ -497,7 +497,7 @@ int ldk_ld_matrix(const int8_t* X, int64_t ld_x, int64_t n_var, const int32_t* r
         set_error("bad sizes");
         return LDK_ERR_ARG;
     }
-    if (estimator < LDK_LDM_R2 || estimator > LDK_LDM_R2_COUNTS) { set_error("unknown estimator"); return LDK_ERR_ARG; }
+    if (estimator < LDK_LDM_R2 || estimator > LDK_LDM_SIGMA_D2_GENO) { set_error("unknown estimator"); return LDK_ERR_ARG; }
     if (n_var > 0 && (!X || !rows)) { set_error("null input pointer"); return LDK_ERR_ARG; }
     if (out && ld_out < n_var) { set_error("ld_out < n_var"); return LDK_ERR_ARG; }
     const size_t need = ld_matrix_workspace(n_var, n_sel);

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "ldk_tc_kernel.cuh"
+#include "ldk_geno_feat.cuh"
 
 namespace ldk {
 
@@ -241,15 +242,234 @@ __global__ void __launch_bounds__(128 + 32 * kLdmEpi, 1)
     }
 }
 
+
+// ---- genotype path: dosage r^2, Rogers-Huff r, sigma_D^2 of genotype pairs ----------------
+
+using LdmGCfg = Cfg<1, true, 0>;               // 128-SNP row blocks, 16-partner tiles
+constexpr int kLdmGEpi = 8;                    // two epilogue warps per TMEM lane quarter
+constexpr int kLdmGPart = LdmGCfg::NJ / 2;     // partners per epilogue warp and tile
+constexpr int kLdmGStride = kLdmGPart + 1;
+
+struct LdmGArgs {
+    const double* mu;   // per SNP: mean dosage over the site's valid individuals
+    const double* var;  // per SNP: sum of squared deviations from it over those individuals
+    double* out;
+    int64_t ld_out;
+    double* sums;
+    double n_ind;       // individuals (Rogers-Huff r: all valid)
+};
+
+// mu and the sum of squared deviations per SNP over the selected rows (ld_statistics.py:
+// 1000-1011); with `strict` a missing call sets LDK_DEVERR_BAD_INPUT (the Rogers-Huff and
+// sigma_D^2 genotype estimators take complete data, ld_statistics.py:389-399).
+__global__ void k_site_moments(const int8_t* __restrict__ X, int64_t ld, int64_t n_var, const int32_t* __restrict__ rows,
+                               int n_rows, int strict, double* __restrict__ mu, double* __restrict__ var,
+                               unsigned* status) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n_var; v += (int64_t)gridDim.x * blockDim.x) {
+        int sum = 0, nv = 0;
+        for (int k = 0; k < n_rows; ++k) {
+            const int8_t x = X[(int64_t)rows[k] * ld + v];
+            if (x >= 0) { sum += x; ++nv; }
+        }
+        if (strict && nv < n_rows) atomicOr(status, LDK_DEVERR_BAD_INPUT);
+        const double m = nv > 0 ? (double)sum / (double)nv : 0.0;
+        double ss = 0.0;
+        for (int k = 0; k < n_rows; ++k) {
+            const int8_t x = X[(int64_t)rows[k] * ld + v];
+            if (x >= 0) ss += ((double)x - m) * ((double)x - m);
+        }
+        mu[v] = m;
+        var[v] = ss;
+    }
+}
+
+template <int EST>
+__global__ void __launch_bounds__(128 + 32 * kLdmGEpi, 1)
+    k_ld_matrix_geno(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcArgs a,
+                     const LdmGArgs m) {
+    using C = LdmGCfg;
+    constexpr int NJ = C::NJ, SP = kLdmGStride;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char* stages = base;
+    double* stile = reinterpret_cast<double*>(base + C::STAGES * C::STAGE_BYTES);  // [kLdmGEpi][32][SP]
+
+    __shared__ __align__(8) uint64_t full_bar[C::STAGES], empty_bar[C::STAGES], tfull[C::NBUF], tempty[C::NBUF];
+    __shared__ __align__(8) uint64_t ifull[kRing], iempty[kRing];
+    __shared__ volatile int ring[kRing];
+    __shared__ uint32_t tmem_base_s;
+    __shared__ volatile int abort_s;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < C::STAGES; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], 1);
+        }
+        for (int b = 0; b < C::NBUF; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], kLdmGEpi);
+        }
+        for (int b = 0; b < kRing; ++b) {
+            mbar_init(&ifull[b], 1);
+            mbar_init(&iempty[b], 1 + kLdmGEpi);
+        }
+        abort_s = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        tmem_alloc(&tmem_base_s, kTmemCols);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base_s;
+    const Pipe pipe{stages, full_bar, empty_bar, tfull, tempty, ifull, iempty, ring, &abort_s};
+    if (warp == 0) run_producer<C>(pipe, &tmA, &tmB, a, lane);
+    else if (warp == 1) run_mma<C, 1>(pipe, tmem, a, lane);
+    if (warp >= 4) {
+        // lane = SNP of the row block (32 per warp); the warp takes half `part` of every tile
+        const int e = warp - 4, quarter = warp & 3, part = e >> 2;
+        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+        double* st = stile + e * 32 * SP;
+        double zsum = 0.0, zcnt = 0.0;
+        uint32_t tcount = 0;
+        for (uint32_t k = 0;; ++k) {
+            const int sl = k % kRing;
+            int item = -1;
+            if (lane == 0) {
+                if (mbar_wait(&ifull[sl], (k / kRing) & 1u, &abort_s, a.status)) {
+                    item = ring[sl];
+                    mbar_arrive(&iempty[sl]);
+                }
+            }
+            item = __shfl_sync(0xffffffffu, item, 0);
+            if (epi_bar_or<kLdmGEpi>(abort_s != 0 || item < 0)) break;
+            const int row0 = a.items[2 * item], row1 = a.items[2 * item + 1];
+            const int jend = a.jmax[row1 - 1];
+            const int n_jt = jend > row0 + 1 ? (jend - row0 + NJ - 1) / NJ : 0;
+            if (n_jt == 0) continue;
+            const int i = row0 + quarter * 32 + lane;
+            const bool row_ok = i < row1;
+            const double mui = row_ok ? m.mu[i] : 0.0, vari = row_ok ? m.var[i] : 0.0;
+            bool ok = true;
+            for (int t = 0; t < n_jt; ++t, ++tcount) {
+                const uint32_t buf = tcount % C::NBUF, tph = (tcount / C::NBUF) & 1u;
+                const int j0 = row0 + t * NJ;
+                if (!mbar_wait(&tfull[buf], tph, &abort_s, a.status)) { ok = false; break; }
+                tc_fence_after();
+#pragma unroll 1
+                for (int cl = 0; cl < kLdmGPart; ++cl) {
+                    const int c = part * kLdmGPart + cl;
+                    uint32_t G[3][4];
+#pragma unroll
+                    for (int x = 0; x < 3; ++x) tmem_ld4(tmem + lane_base + buf * C::COLS + x * C::N + 4 * c, G[x]);
+                    const int j = j0 + c;
+                    const double muj = j < jend ? m.mu[j] : 0.0, varj = j < jend ? m.var[j] : 0.0;
+                    tmem_wait4<3>(G);
+                    if (cl == kLdmGPart - 1) {
+                        tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(&tempty[buf]);
+                    }
+                    const bool valid = row_ok && j > i && j < jend;
+                    double val = 0.0;
+                    if (valid) {
+                        // G[x][y]: plane x of SNP i . plane y of SNP j (0: g == 1, 1: g == 2, 2: valid)
+                        const int n11 = (int)G[0][0], n12 = (int)G[0][1], n21 = (int)G[1][0], n22 = (int)G[1][1];
+                        const int n10 = (int)G[0][2] - n11 - n12, n20 = (int)G[1][2] - n21 - n22;
+                        const int n01 = (int)G[2][0] - n11 - n21, n02 = (int)G[2][1] - n12 - n22;
+                        const int nv = (int)G[2][2];
+                        if constexpr (EST == 3 || EST == 4) {
+                            const double sxy = (double)(n11 + 2 * (n12 + n21) + 4 * n22);
+                            if constexpr (EST == 3) {
+                                // centred dosages zeroed where missing (ld_statistics.py:1000-1018)
+                                const double sx = (double)((n10 + n11 + n12) + 2 * (n20 + n21 + n22));
+                                const double sy = (double)((n01 + n11 + n21) + 2 * (n02 + n12 + n22));
+                                const double cov = sxy - muj * sx - mui * sy + mui * muj * (double)nv;
+                                const double vv = vari * varj;
+                                val = vv > 0.0 ? (cov * cov) / vv : 0.0;
+                                zsum += val;
+                                zcnt += 1.0;
+                            } else {
+                                // ld_statistics.py:392-437
+                                const double cov = sxy - m.n_ind * mui * muj;
+                                const double den = sqrt(vari * varj);
+                                if (den > 0.0) {
+                                    val = cov / den;
+                                    zsum += val * val;
+                                    zcnt += 1.0;
+                                } else {
+                                    val = CUDART_NAN;
+                                }
+                            }
+                        } else {
+                            // DD over pi2 numerators of one population (genotype_kernels.py:91-170)
+                            const int n00 = nv - n01 - n02 - n10 - n11 - n12 - n20 - n21 - n22;
+                            const double cd[9] = {(double)n00, (double)n01, (double)n02, (double)n10, (double)n11,
+                                                  (double)n12, (double)n20, (double)n21, (double)n22};
+                            GenoFeat<double> f;
+                            geno_set_counts(f, cd);
+                            f.n = (double)nv;
+                            geno_features<double, 1>(f);
+                            if (nv >= 4 && f.PI1 > 0.0) {
+                                val = f.DD1 / f.PI1;
+                                zsum += val;
+                                zcnt += 1.0;
+                            } else {
+                                val = CUDART_NAN;
+                            }
+                        }
+                    }
+                    st[lane * SP + cl] = val;
+                }
+                __syncwarp();
+                if (m.out) {
+                    const int gi0 = row0 + quarter * 32, gj0 = j0 + part * kLdmGPart;
+                    for (int idx = lane; idx < 32 * kLdmGPart; idx += 32) {  // rows: upper triangle
+                        const int r = idx / kLdmGPart, cc = idx % kLdmGPart, gi = gi0 + r, gj = gj0 + cc;
+                        if (gi < row1 && gj > gi && gj < jend) m.out[(int64_t)gi * m.ld_out + gj] = st[r * SP + cc];
+                    }
+                    for (int idx = lane; idx < 32 * kLdmGPart; idx += 32) {  // columns: lower triangle
+                        const int r = idx % 32, cc = idx / 32, gi = gi0 + r, gj = gj0 + cc;
+                        if (gi < row1 && gj > gi && gj < jend) m.out[(int64_t)gj * m.ld_out + gi] = st[r * SP + cc];
+                    }
+                }
+                __syncwarp();
+            }
+            (void)ok;
+        }
+        if (m.sums) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                zsum += __shfl_xor_sync(0xffffffffu, zsum, o);
+                zcnt += __shfl_xor_sync(0xffffffffu, zcnt, o);
+            }
+            if (lane == 0) {
+                atomicAdd(&m.sums[0], zsum);
+                atomicAdd(&m.sums[1], zcnt);
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem, kTmemCols);
+    }
+}
+
 struct LdmLayout {
-    size_t status = 0, jmax = 0, items = 0, planes = 0, psite = 0, total = 0;
+    size_t status = 0, jmax = 0, items = 0, planes = 0, psite = 0, var = 0, total = 0;
     int n_items = 0, ktot = 0;
 };
 
-LdmLayout ldm_layout(int64_t n_var, int32_t n_sel) {
+LdmLayout ldm_layout(int64_t n_var, int32_t n_sel, bool geno) {
     LdmLayout L;
     L.ktot = (int)(((n_sel + 31) / 32 * 32 + 127) / 128 * 128);
-    L.n_items = (int)((n_var + LdmCfg::ROWS - 1) / LdmCfg::ROWS);
+    const int rows = geno ? LdmGCfg::ROWS : LdmCfg::ROWS;
+    L.n_items = (int)((n_var + rows - 1) / rows);
     auto up = [](size_t x, size_t a) { return (x + a - 1) / a * a; };
     size_t off = 256;
     L.jmax = off;
@@ -257,11 +477,30 @@ LdmLayout ldm_layout(int64_t n_var, int32_t n_sel) {
     L.items = off;
     off = up(off + (size_t)L.n_items * 8, 1024);
     L.planes = off;
-    off = up(off + (size_t)n_var * 2 * L.ktot, 256);
+    off = up(off + (size_t)n_var * (geno ? 4 : 2) * L.ktot, 256);
     L.psite = off;
+    off = up(off + (size_t)n_var * 8, 256);
+    L.var = off;
     off = up(off + (size_t)n_var * 8, 256);
     L.total = off;
     return L;
+}
+
+template <int EST>
+cudaError_t launch_ldm_geno(const CUtensorMap& mA, const CUtensorMap& mB, const TcArgs& a, const LdmGArgs& m,
+                            int n_items, cudaStream_t s) {
+    using C = LdmGCfg;
+    size_t smem = 1024 + (size_t)C::STAGES * C::STAGE_BYTES + (size_t)kLdmGEpi * 32 * kLdmGStride * sizeof(double);
+    if (smem < kMinSmem) smem = kMinSmem;
+    if (smem > kMaxSmem) return cudaErrorInvalidConfiguration;
+    cudaError_t e = cudaFuncSetAttribute(k_ld_matrix_geno<EST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = n_items < sms ? n_items : sms;
+    k_ld_matrix_geno<EST><<<grid, 128 + 32 * kLdmGEpi, smem, s>>>(mA, mB, a, m);
+    return cudaGetLastError();
 }
 
 template <int EST>
@@ -282,41 +521,51 @@ cudaError_t launch_ldm(const CUtensorMap& mA, const CUtensorMap& mB, const TcArg
 
 }  // namespace
 
-size_t ld_matrix_workspace(int64_t n_var, int32_t n_sel) { return ldm_layout(n_var, n_sel).total; }
+size_t ld_matrix_workspace(int64_t n_var, int32_t n_sel) { return ldm_layout(n_var, n_sel, true).total; }
 
 // Enqueues the all-pairs LD of the n_sel selected rows of X (see ldk_ld_matrix).
 cudaError_t launch_ld_matrix(const int8_t* X, int64_t ld_x, int64_t n_var, const int32_t* rows, int32_t n_sel,
                              int estimator, double* out, int64_t ld_out, double* sums, unsigned char* ws,
                              unsigned* status, cudaStream_t s) {
-    const LdmLayout L = ldm_layout(n_var, n_sel);
+    const bool geno = estimator >= 3;
+    const LdmLayout L = ldm_layout(n_var, n_sel, geno);
     cudaError_t e;
     int32_t* jmax = reinterpret_cast<int32_t*>(ws + L.jmax);
     int32_t* items = reinterpret_cast<int32_t*>(ws + L.items);
     uint8_t* planes = ws + L.planes;
     double* psite = reinterpret_cast<double*>(ws + L.psite);
+    double* svar = reinterpret_cast<double*>(ws + L.var);
     if (sums && (e = cudaMemsetAsync(sums, 0, 2 * sizeof(double), s)) != cudaSuccess) return e;
     if (out && n_var > 0) {
-        k_fill_diag<<<(unsigned)((n_var + 255) / 256), 256, 0, s>>>(out, ld_out, n_var, estimator == 2 ? std::nan("") : 0.0);
+        const bool nan_diag = estimator == LDK_LDM_R2_COUNTS || estimator >= LDK_LDM_ROGERS_HUFF_R;
+        k_fill_diag<<<(unsigned)((n_var + 255) / 256), 256, 0, s>>>(out, ld_out, n_var, nan_diag ? std::nan("") : 0.0);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     if (n_var < 2) return cudaSuccess;
     // every SNP's partner range is the rest of the set
     k_fill_int<<<(unsigned)((n_var + 255) / 256), 256, 0, s>>>(jmax, n_var, (int32_t)n_var);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const int rows_per_block = geno ? LdmGCfg::ROWS : LdmCfg::ROWS;
     std::vector<int32_t> it;
     it.reserve((size_t)L.n_items * 2);
-    for (int64_t r0 = 0; r0 < n_var; r0 += LdmCfg::ROWS) {  // most partners first
+    for (int64_t r0 = 0; r0 < n_var; r0 += rows_per_block) {  // most partners first
         it.push_back((int32_t)r0);
-        it.push_back((int32_t)std::min<int64_t>(r0 + LdmCfg::ROWS, n_var));
+        it.push_back((int32_t)std::min<int64_t>(r0 + rows_per_block, n_var));
     }
     if ((e = cudaMemcpyAsync(items, it.data(), it.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s)) != cudaSuccess)
         return e;
-    if (estimator == 0) {
+    if (estimator == LDK_LDM_R2) {
         k_site_freq<<<(unsigned)((n_var + 255) / 256), 256, 0, s>>>(X, ld_x, n_var, rows, n_sel, psite);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (geno) {
+        k_site_moments<<<(unsigned)((n_var + 255) / 256), 256, 0, s>>>(
+            X, ld_x, n_var, rows, n_sel, estimator != LDK_LDM_DIPLOID_R2, psite, svar, status);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     // the indicator planes of the selected rows, as for a one-population parse
     ldk_parse_t d{};
+    d.genotypes = geno ? 1 : 0;
     d.X = X;
     d.ld_x = ld_x;
     d.n_var = n_var;
@@ -326,8 +575,8 @@ cudaError_t launch_ld_matrix(const int8_t* X, int64_t ld_x, int64_t n_var, const
     for (int p = 1; p <= LDK_MAX_POPS; ++p) d.pop_offsets[p] = n_sel;
     ParseShape sh{};
     sh.P = 1;
-    sh.genotypes = 0;
-    sh.planes = 2;
+    sh.genotypes = geno ? 1 : 0;
+    sh.planes = geno ? 4 : 2;
     sh.ktot = L.ktot;
     for (int p = 0; p <= LDK_MAX_POPS; ++p) sh.kofs[p] = p == 0 ? 0 : (n_sel + 31) / 32 * 32;
     sh.max_n = n_sel;
@@ -336,8 +585,10 @@ cudaError_t launch_ld_matrix(const int8_t* X, int64_t ld_x, int64_t n_var, const
     w.hv = planes;
     if ((e = launch_prep_planes(&d, w, sh, s)) != cudaSuccess) return e;
     CUtensorMap mA, mB;
-    if (!make_map(&mA, planes, n_var, L.ktot, 2, 2, LdmCfg::ROWS) ||
-        !make_map(&mB, planes, n_var, L.ktot, 2, 2, LdmCfg::NJ))
+    if (geno ? (!make_map(&mA, planes, n_var, L.ktot, 4, 1, LdmGCfg::ROWS) ||
+                !make_map(&mB, planes, n_var, L.ktot, 4, 4, LdmGCfg::NJ))
+             : (!make_map(&mA, planes, n_var, L.ktot, 2, 2, LdmCfg::ROWS) ||
+                !make_map(&mB, planes, n_var, L.ktot, 2, 2, LdmCfg::NJ)))
         return cudaErrorInvalidValue;
     TcArgs a{};
     a.jmax = jmax;
@@ -347,10 +598,18 @@ cudaError_t launch_ld_matrix(const int8_t* X, int64_t ld_x, int64_t n_var, const
     a.nkc = L.ktot / kKChunk;
     for (int p = 0; p <= LDK_MAX_POPS; ++p) a.kofs[p] = sh.kofs[p];
     a.status = status;
+    if (geno) {
+        LdmGArgs g{psite, svar, out, ld_out, sums, (double)n_sel};
+        switch (estimator) {
+            case LDK_LDM_DIPLOID_R2: return launch_ldm_geno<3>(mA, mB, a, g, L.n_items, s);
+            case LDK_LDM_ROGERS_HUFF_R: return launch_ldm_geno<4>(mA, mB, a, g, L.n_items, s);
+            default: return launch_ldm_geno<5>(mA, mB, a, g, L.n_items, s);
+        }
+    }
     LdmArgs m{psite, out, ld_out, sums};
     switch (estimator) {
-        case 0: return launch_ldm<0>(mA, mB, a, m, L.n_items, s);
-        case 1: return launch_ldm<1>(mA, mB, a, m, L.n_items, s);
+        case LDK_LDM_R2: return launch_ldm<0>(mA, mB, a, m, L.n_items, s);
+        case LDK_LDM_SIGMA_D2: return launch_ldm<1>(mA, mB, a, m, L.n_items, s);
         default: return launch_ldm<2>(mA, mB, a, m, L.n_items, s);
     }
 }

@@ -169,10 +169,17 @@ class HaplotypeMatrix:
     def pairwise_r2(self, estimator="r2"):
         """(n_variants, n_variants) float64 pairwise r^2 on the GPU
         (haplotype_matrix.py:1138-1175); ``estimator='sigma_d2'`` gives the unbiased
-        sigma_D^2 matrix instead.  Rogers-Huff dosage r^2 is not provided here."""
-        from .ld_matrix import ld_matrix
+        sigma_D^2 matrix instead, ``'rogers_huff'`` the Rogers-Huff r^2 of paired
+        haplotypes (NaN set to 0)."""
+        from .ld_matrix import dosages, ld_matrix
+        if estimator == "rogers_huff":  # haplotype_matrix.py:1159-1165: squared, NaN -> 0, diagonal 0
+            r = ld_matrix(dosages(self), estimator="rogers_huff_r")[0]
+            r2 = r * r
+            r2 = r2.nan_to_num(nan=0.0)
+            r2.fill_diagonal_(0.0)
+            return r2
         if estimator not in ("r2", "sigma_d2"):
-            raise ValueError(f"Unknown estimator: {estimator!r} (expected 'r2' or 'sigma_d2')")
+            raise ValueError(f"Unknown estimator: {estimator!r} (expected 'r2', 'rogers_huff' or 'sigma_d2')")
         self.transfer_to_gpu()
         return ld_matrix(self.haplotypes, estimator=estimator)[0]
 

@@ -13,7 +13,8 @@ import numpy as np
 
 from . import _lib
 
-ESTIMATORS = {"r2": 0, "sigma_d2": 1, "r2_counts": 2}
+ESTIMATORS = {"r2": 0, "sigma_d2": 1, "r2_counts": 2,                          # haplotypes
+              "diploid_r2": 3, "rogers_huff_r": 4, "sigma_d2_geno": 5}           # genotypes
 
 
 def _hap_tensor(hap, torch):
@@ -27,7 +28,8 @@ def ld_matrix(hap, rows=None, estimator="r2", matrix=True, reduce=False, stream=
 
     Returns ``(M, sums)``: ``M`` the (n_var, n_var) float64 matrix (or None) and ``sums``
     the float64 tensor [sum over pairs i < j entering ZnS's mean, their count] (or None).
-    ``estimator``: "r2" (pairwise_r2), "sigma_d2" or "r2_counts" (see ``ldk_ld_matrix``)."""
+    ``estimator``: haplotypes "r2" (pairwise_r2), "sigma_d2", "r2_counts"; genotypes
+    "diploid_r2", "rogers_huff_r", "sigma_d2_geno" (see ``ldk_ld_matrix``)."""
     torch = _lib.require_cuda()
     lib = _lib.load()
     X = _hap_tensor(hap, torch)
@@ -156,3 +158,90 @@ def windowed_r_squared(hap, positions, bp_bins, percentile=50, rows=None):
         if cnt[k]:
             res[k] = torch.quantile(vals[b == k], q).cpu().numpy()
     return (res[:, 0] if res.shape[1] == 1 else res), cnt
+
+
+# ---------------------------------------------------------------------------
+# genotype input (ld_statistics.py:371-531, 973-1021; ld_statistics_genotype.py:1518-1598)
+# ---------------------------------------------------------------------------
+
+
+def dosages(matrix):
+    """(n_individuals, n_variants) int8 dosages of a GenotypeMatrix, or of a HaplotypeMatrix
+    with adjacent haplotypes paired (ld_statistics.py:371-409); missing calls raise, as in
+    the reference's Rogers-Huff and sigma_D^2 genotype functions."""
+    torch = _lib.require_cuda()
+    from .genotype_matrix import GenotypeMatrix
+    from .haplotype_matrix import HaplotypeMatrix
+    if isinstance(matrix, HaplotypeMatrix):
+        matrix.transfer_to_gpu()
+        hap = matrix.haplotypes
+        if bool((hap < 0).any()):
+            raise ValueError("input HaplotypeMatrix contains missing values (-1); drop or impute missing sites first")
+        if hap.shape[0] % 2:
+            raise ValueError(f"HaplotypeMatrix has an odd number of haplotypes ({hap.shape[0]}); cannot pair into diploids")
+        return (hap[0::2] + hap[1::2]).to(torch.int8).contiguous()
+    if isinstance(matrix, GenotypeMatrix):
+        matrix.transfer_to_gpu()
+        g = matrix.genotypes
+        if bool((g < 0).any()):
+            raise ValueError("input GenotypeMatrix contains missing values (-1); drop or impute missing sites first")
+        return g.to(torch.int8).contiguous()
+    raise TypeError(f"expected HaplotypeMatrix or GenotypeMatrix; got {type(matrix).__name__}")
+
+
+def _condensed(M):
+    torch = _lib.require_cuda()
+    m = M.shape[0]
+    iu = torch.triu_indices(m, m, offset=1, device=M.device)
+    return M[iu[0], iu[1]]
+
+
+def rogers_huff_r(matrix):
+    """Condensed (upper triangle, row-major pair order) Rogers-Huff r of the dosages
+    (ld_statistics.py:492-521); NaN where a site is constant."""
+    return _condensed(ld_matrix(dosages(matrix), estimator="rogers_huff_r")[0])
+
+
+def rogers_huff_r_squared(matrix):
+    """``rogers_huff_r(matrix) ** 2`` (ld_statistics.py:524-531)."""
+    return rogers_huff_r(matrix) ** 2
+
+
+def sigma_d2_geno(matrix, idx_i=None, idx_j=None):
+    """Unbiased sigma_D^2 of genotype pairs (ld_statistics_genotype.py:1518-1598): all pairs
+    i < j in condensed order, or the given pairs; NaN where pi2 is not positive or fewer
+    than 4 individuals."""
+    torch = _lib.require_cuda()
+    M = ld_matrix(dosages(matrix), estimator="sigma_d2_geno")[0]
+    if idx_i is None and idx_j is None:
+        return _condensed(M)
+    if idx_i is None or idx_j is None:
+        raise ValueError("idx_i and idx_j must be provided together")
+    ii = torch.as_tensor(np.asarray(idx_i), dtype=torch.int64, device="cuda")
+    jj = torch.as_tensor(np.asarray(idx_j), dtype=torch.int64, device="cuda")
+    if ii.shape != jj.shape:
+        raise ValueError("idx_i and idx_j must have the same shape")
+    return M[ii, jj]
+
+
+def diploid_r2_matrix(geno, missing_data="include"):
+    """Dosage r^2 matrix of a genotype array with missing calls allowed
+    (ld_statistics.py:973-1021; 'exclude' first drops sites with a missing call)."""
+    torch = _lib.require_cuda()
+    X = _hap_tensor(geno, torch)
+    if missing_data == "exclude":
+        X = X[:, (X < 0).sum(0) == 0].contiguous()
+    return ld_matrix(X, estimator="diploid_r2")[0]
+
+
+def zns_diploid(geno, missing_data="include"):
+    """ZnS of a genotype array: mean off-diagonal dosage r^2 (ld_statistics.py:720-735)."""
+    torch = _lib.require_cuda()
+    X = _hap_tensor(geno, torch)
+    if missing_data == "exclude":
+        X = X[:, (X < 0).sum(0) == 0].contiguous()
+    m = X.shape[1]
+    if m < 2:
+        return 0.0
+    _, S = ld_matrix(X, estimator="diploid_r2", matrix=False, reduce=True)
+    return S[0].item() / (m * (m - 1) / 2)

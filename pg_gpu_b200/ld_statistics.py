@@ -144,8 +144,11 @@ def zns(r2_matrix_or_matrix, missing_data="include", estimator="auto"):
         return ld_matrix.zns(r2_matrix_or_matrix.haplotypes, missing_data, estimator)
     if estimator == "sigma_d2":
         raise ValueError("estimator='sigma_d2' requires a HaplotypeMatrix, not a pre-computed r^2 array")
-    if hasattr(r2_matrix_or_matrix, "genotypes"):
-        raise NotImplementedError("diploid r^2 matrices are not provided; pass a HaplotypeMatrix or an r^2 array")
+    if hasattr(r2_matrix_or_matrix, "genotypes"):  # GenotypeMatrix: dosage r^2 (ld_statistics.py:926-972)
+        if estimator not in ("auto", "r2", "rogers_huff"):
+            raise ValueError(f"Unknown estimator: {estimator!r}")
+        r2_matrix_or_matrix.transfer_to_gpu()
+        return ld_matrix.zns_diploid(r2_matrix_or_matrix.genotypes, missing_data)
     torch = _lib.require_cuda()
     M = torch.as_tensor(r2_matrix_or_matrix, dtype=torch.float64, device="cuda")
     m = M.shape[0]
@@ -164,6 +167,22 @@ def omega(r2_matrix_or_matrix, missing_data="include", estimator="auto"):
         return ld_matrix.omega(r2_matrix_or_matrix.haplotypes, missing_data, estimator)
     if estimator == "sigma_d2":
         raise ValueError("estimator='sigma_d2' requires a HaplotypeMatrix")
-    if hasattr(r2_matrix_or_matrix, "genotypes"):
-        raise NotImplementedError("diploid r^2 matrices are not provided; pass a HaplotypeMatrix or an r^2 array")
+    if hasattr(r2_matrix_or_matrix, "genotypes"):  # GenotypeMatrix: dosage r^2 (ld_statistics.py:926-972)
+        if estimator not in ("auto", "r2", "rogers_huff"):
+            raise ValueError(f"Unknown estimator: {estimator!r}")
+        r2_matrix_or_matrix.transfer_to_gpu()
+        return ld_matrix.omega_from_matrix(ld_matrix.diploid_r2_matrix(r2_matrix_or_matrix.genotypes, missing_data))
     return ld_matrix.omega_from_matrix(r2_matrix_or_matrix)
+
+
+def rogers_huff_r(matrix, tile_size=None):
+    """Condensed Rogers-Huff r of a HaplotypeMatrix (paired haplotypes) or GenotypeMatrix
+    (ld_statistics.py:492-521); ``tile_size`` is accepted for call compatibility."""
+    from . import ld_matrix
+    return ld_matrix.rogers_huff_r(matrix)
+
+
+def rogers_huff_r_squared(matrix, tile_size=None):
+    """Squared ``rogers_huff_r`` (ld_statistics.py:524-531)."""
+    from . import ld_matrix
+    return ld_matrix.rogers_huff_r_squared(matrix)

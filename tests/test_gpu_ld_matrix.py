@@ -82,3 +82,53 @@ def test_reduce_only_and_errors():
     lib = _lib.load()
     assert lib.ldk_ld_matrix(None, 0, 5, None, 1, 0, None, 0, None, None, 0, None) == _lib.LDK_ERR_ARG
     assert lib.ldk_ld_matrix(None, 10, 10, None, 3, 7, None, 10, None, None, 0, None) == _lib.LDK_ERR_ARG
+
+
+def test_genotype_all_pairs_match_reference(g):
+    from pg_gpu_b200 import genotype_matrix, ld_statistics_genotype
+    gm = genotype_matrix.GenotypeMatrix(g["geno"], g["pos"])
+    np.testing.assert_allclose(ld_statistics.rogers_huff_r(gm).cpu().numpy(), g["rogers_huff_r"], rtol=1e-12,
+                               atol=1e-15, equal_nan=True)
+    np.testing.assert_allclose(ld_statistics_genotype.sigma_d2_geno(gm).cpu().numpy(), g["sigma_d2_geno"],
+                               rtol=1e-12, atol=1e-15, equal_nan=True)
+    gmm = genotype_matrix.GenotypeMatrix(g["geno_missing"], g["pos"])
+    np.testing.assert_allclose(ld_matrix.diploid_r2_matrix(g["geno_missing"]).cpu().numpy(), g["diploid_r2"],
+                               rtol=1e-11, atol=1e-14)
+    np.testing.assert_allclose(ld_statistics.zns(gmm), g["zns_diploid"], rtol=1e-11)
+    np.testing.assert_allclose(ld_statistics.omega(gmm), g["omega_diploid"], rtol=1e-11)
+    with pytest.raises(ValueError, match="missing"):
+        ld_statistics.rogers_huff_r(gmm)
+
+
+@pytest.mark.parametrize("n_ind,m", [(150, 300), (33, 129), (5, 40)])
+def test_genotype_estimators_match_oracle(n_ind, m):
+    rng = np.random.default_rng(n_ind * 7 + m)
+    geno = (rng.random((n_ind, m)) < rng.uniform(0.05, 0.6, m)).astype(np.int8) + \
+        (rng.random((n_ind, m)) < rng.uniform(0.05, 0.6, m)).astype(np.int8)
+    geno[:, 3] = 1  # constant site
+    iu = np.triu_indices(m, k=1)
+    M, _ = ld_matrix.ld_matrix(geno, estimator="rogers_huff_r")
+    np.testing.assert_allclose(M.cpu().numpy()[iu], O.rogers_huff_r(geno), rtol=1e-11, atol=1e-14, equal_nan=True)
+    M, _ = ld_matrix.ld_matrix(geno, estimator="sigma_d2_geno")
+    np.testing.assert_allclose(M.cpu().numpy()[iu], O.sigma_d2_geno(geno), rtol=1e-11, atol=1e-14, equal_nan=True)
+    gm = geno.copy()
+    gm[rng.random(gm.shape) < 0.05] = -1
+    M, S = ld_matrix.ld_matrix(gm, estimator="diploid_r2", reduce=True)
+    want = O.diploid_r2_matrix(gm)
+    np.testing.assert_allclose(M.cpu().numpy(), want, rtol=1e-10, atol=1e-13)
+    np.testing.assert_allclose(S.cpu().numpy(), [np.triu(want, 1).sum(), m * (m - 1) / 2], rtol=1e-10)
+    # complete-data estimators reject missing calls through the device status
+    with pytest.raises(_lib.LdkError):
+        ld_matrix.ld_matrix(gm, estimator="rogers_huff_r")
+
+
+def test_haplotype_rogers_huff_pairwise():
+    rng = np.random.default_rng(12)
+    hap = (rng.random((40, 50)) < 0.4).astype(np.int8)
+    hm = haplotype_matrix.HaplotypeMatrix(hap, np.arange(50) * 10)
+    r = O.rogers_huff_r(hap[0::2] + hap[1::2])
+    want = np.zeros((50, 50))
+    iu = np.triu_indices(50, k=1)
+    want[iu] = np.nan_to_num(r ** 2)
+    want = want + want.T
+    np.testing.assert_allclose(hm.pairwise_r2("rogers_huff").cpu().numpy(), want, rtol=1e-11, atol=1e-14)
