@@ -213,7 +213,8 @@ def main():
                     help="time the all-pairs LD kernel (ldk_ld_matrix) instead of the binned parse")
     ap.add_argument("--snps", type=int, default=24576, help="--all-pairs: SNPs in the set")
     ap.add_argument("--haplotypes", type=int, default=200, help="--all-pairs: haplotypes")
-    ap.add_argument("--estimator", choices=["r2", "sigma_d2", "r2_counts"], default="r2")
+    ap.add_argument("--estimator", choices=["r2", "sigma_d2", "r2_counts", "diploid_r2", "rogers_huff_r",
+                                            "sigma_d2_geno"], default="r2")
     ap.add_argument("--reduce-only", action="store_true", help="--all-pairs: ZnS sums only, no matrix")
     args = ap.parse_args()
 
@@ -477,13 +478,20 @@ def run_all_pairs(args):
     lib = _lib.load()
     rng = np.random.default_rng(6)
     m, n = args.snps, args.haplotypes
-    hap, _pos = synth.haplotype_region(rng, [n], m, m * 100, 0.01)
+    est = ld_matrix.ESTIMATORS[args.estimator]
+    geno = est >= 3
+    # genotype estimators: dosages of paired haplotypes (complete data where the estimator needs it)
+    hap, _pos = synth.haplotype_region(rng, [2 * n if geno else n], m, m * 100,
+                                       0.0 if args.estimator in ("rogers_huff_r", "sigma_d2_geno") else 0.01)
+    if geno:
+        g = (np.maximum(hap[0::2], 0) + np.maximum(hap[1::2], 0)).astype(np.int8)
+        g[(hap[0::2] < 0) | (hap[1::2] < 0)] = -1
+        hap = g
     X = torch.as_tensor(np.ascontiguousarray(hap), device="cuda")
     R = torch.arange(n, dtype=torch.int32, device="cuda")
     M = None if args.reduce_only else torch.empty((m, m), dtype=torch.float64, device="cuda")
     S = torch.zeros(2, dtype=torch.float64, device="cuda")
     wsb = torch.empty(int(lib.ldk_ld_matrix_workspace_size(m, n)), dtype=torch.uint8, device="cuda")
-    est = ld_matrix.ESTIMATORS[args.estimator]
 
     def step():
         _lib.check(lib.ldk_ld_matrix(_lib.ptr(X), m, m, _lib.ptr(R), n, est, _lib.ptr(M), m, _lib.ptr(S),
@@ -509,7 +517,7 @@ def run_all_pairs(args):
         roof = {"bound": "hbm", "achieved": bytes_ / (ms / 1e3) / 1e9, "peak": pk_d["hbm_gbs"], "unit": "GB/s",
                 "peak_source": f"{pk_kind} copy bandwidth", "algorithmic_bytes": bytes_}
     else:
-        ops = 8 * n * pairs
+        ops = (18 if geno else 8) * n * pairs
         roof = {"bound": "tensor", "achieved": ops / (ms / 1e3) / 1e12, "peak": probe_i8 / 1e12,
                 "unit": "TOP/s (INT8, MAC=2)", "peak_source": "measured in this run: ldk_probe_peaks"}
     roof["frac"] = roof["achieved"] / roof["peak"]
@@ -519,10 +527,10 @@ def run_all_pairs(args):
         "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8 counts / s32 accumulate / f64 values",
         "data": "synthetic (seeded founder mosaics, 1% missing)",
-        "config": {"workload": f"all-pairs {args.estimator}, {m} SNPs x {n} haplotypes",
+        "config": {"workload": f"all-pairs {args.estimator}, {m} SNPs x {n} {'individuals' if geno else 'haplotypes'}",
                    "matrix": M is not None, "pairs": pairs, "l2": "matrix larger than L2" if M is not None else
                    "reduction only"},
-        "roofline": roof, "gpu_launches": int(args.steps * ((M is not None) + (est == 0) + 3)),
+        "roofline": roof, "gpu_launches": int(args.steps * ((M is not None) + (est == 0) + geno + 3)),
         "clocks": clk.summary()}),
         flush=True)
 
