@@ -80,6 +80,9 @@ struct Cfg {
     static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
     static constexpr int NS = HapNStats<P>::value;
     static constexpr int SLOTS = GENO ? 4 : 2;                         // bootstrap blocks staged per row block
+    // epilogue warps: one per TMEM lane quarter, or -- for one population, whose epilogue
+    // needs few registers -- two, each taking half of every partner tile
+    static constexpr int EPI = P == 1 ? 8 : 4;
     static_assert(NBUF * COLS <= kTmemCols, "TMEM budget");
     static_assert(N % 16 == 0 && N <= 256, "MMA N");
 };
@@ -356,16 +359,17 @@ LDK_DEV void run_mma(const Pipe& S, uint32_t tmem, const TcArgs& a, int lane) {
 }
 
 template <int P, typename T, bool PRIV, bool GENO, int V>
-__global__ void __launch_bounds__(128 + 32 * kEpi, 1)
+__global__ void __launch_bounds__(128 + 32 * Cfg<P, GENO, V>::EPI, 1)
     k_parse_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcArgs a) {
     using C = Cfg<P, GENO, V>;
     constexpr int NS = C::NS;
+    constexpr int EPI = C::EPI;
     constexpr int SLOTS = C::SLOTS;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int nb = a.edges.n_bins;
     unsigned char* stages = base;
-    constexpr int NCOPY = PRIV ? kEpi : 1;  // staging copies: one per epilogue warp, or shared
+    constexpr int NCOPY = PRIV ? EPI : 1;  // staging copies: one per epilogue warp, or shared
     double* sacc = reinterpret_cast<double*>(base + C::STAGES * C::STAGE_BYTES);  // [NCOPY][SLOTS][nb][NS+1]
     unsigned* scnt = reinterpret_cast<unsigned*>(sacc + NCOPY * SLOTS * nb * (NS + 1));  // [NCOPY][SLOTS][nb][2]
     double4* rtab = reinterpret_cast<double4*>(scnt + ((NCOPY * SLOTS * nb * 2 + 7) & ~7));  // [max_n + 1]
@@ -385,11 +389,11 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
         }
         for (int b = 0; b < C::NBUF; ++b) {
             mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], kEpi);
+            mbar_init(&tempty[b], EPI);
         }
         for (int b = 0; b < kRing; ++b) {
             mbar_init(&ifull[b], 1);
-            mbar_init(&iempty[b], 1 + kEpi);  // the MMA issuer and every epilogue warp
+            mbar_init(&iempty[b], 1 + EPI);  // the MMA issuer and every epilogue warp
         }
         abort_s = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -415,13 +419,18 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
         const int e = warp - 4;
         const int L = (warp & 3) * 32 + lane;
         // haplotype rows: lanes 2r, 2r+1 share SNP r and split its partners by parity;
-        // genotype rows: lane L is SNP L and takes every partner
+        // genotype rows: lane L is SNP L and takes every partner.  With two warps per lane
+        // quarter each takes a contiguous half of every partner tile, so every lane still
+        // sees its partners in increasing order.
         const int r = GENO ? L : L >> 1, role = GENO ? 0 : L & 1;
         const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
         const int stage_n = SLOTS * nb * (NS + 1);
         double* my_sacc = sacc + (PRIV ? e * stage_n : 0);
         unsigned* my_scnt = scnt + (PRIV ? e * SLOTS * nb * 2 : 0);
         constexpr int STEPS = GENO ? C::NJ : C::NJ / 2;   // TMEM reads per tile
+        constexpr int PARTS = EPI / 4;                    // epilogue warps per lane quarter
+        constexpr int MY_STEPS = STEPS / PARTS;           // ... each reading a contiguous share
+        const int part = e >> 2;
         constexpr int CREGS = (C::NJ + 31) / 32;          // partner coordinates per lane
         uint32_t tcount = 0;
         for (uint32_t k = 0;; ++k) {
@@ -434,7 +443,7 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
                 }
             }
             item = __shfl_sync(0xffffffffu, item, 0);
-            if (epi_bar_or<kEpi>(abort_s != 0 || item < 0)) break;
+            if (epi_bar_or<EPI>(abort_s != 0 || item < 0)) break;
             const int row0 = a.items[2 * item], row1 = a.items[2 * item + 1];
             const int jend = a.jmax[row1 - 1];
             const int n_jt = jend > row0 + 1 ? (jend - row0 + C::NJ - 1) / C::NJ : 0;
@@ -508,7 +517,8 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
                 // registers.  Haplotypes: two partners per step, 4 columns per population.
                 // Genotypes: one partner per step, 4 columns per region and population.
 #pragma unroll 1
-                for (int q = 0; q < STEPS; ++q) {
+                for (int qq = 0; qq < MY_STEPS; ++qq) {
+                    const int q = part * MY_STEPS + qq;
                     uint32_t v[P][C::REGIONS][4];
 #pragma unroll
                     for (int p = 0; p < P; ++p)
@@ -524,7 +534,7 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
                     const double cj = __shfl_sync(0xffffffffu, csrc, jj & 31);
 #pragma unroll
                     for (int p = 0; p < P; ++p) tmem_wait4<C::REGIONS>(v[p]);
-                    if (q == STEPS - 1) {
+                    if (qq == MY_STEPS - 1) {
                         tc_fence_before();
                         __syncwarp();
                         if (lane == 0) mbar_arrive(&tempty[buf]);
@@ -605,12 +615,12 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
             flush(cur >= 0 && cur < nb && np > 0);
             (void)ok;
             // staging -> global, once per row block
-            epi_bar<kEpi>();
+            epi_bar<EPI>();
             const int et = threadIdx.x - 128;
-            for (int idx = et; idx < stage_n; idx += 32 * kEpi) {
+            for (int idx = et; idx < stage_n; idx += 32 * EPI) {
                 double val = 0.0;
 #pragma unroll
-                for (int w = 0; w < (PRIV ? kEpi : 1); ++w) {
+                for (int w = 0; w < (PRIV ? EPI : 1); ++w) {
                     val += sacc[w * stage_n + idx];
                     sacc[w * stage_n + idx] = 0.0;
                 }
@@ -623,10 +633,10 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
                     else atomicAdd(&a.r2_sums[(int64_t)blk * nb + bb], val);
                 }
             }
-            for (int idx = et; idx < SLOTS * nb; idx += 32 * kEpi) {
+            for (int idx = et; idx < SLOTS * nb; idx += 32 * EPI) {
                 unsigned long long c0 = 0, c1 = 0;
 #pragma unroll
-                for (int w = 0; w < (PRIV ? kEpi : 1); ++w) {
+                for (int w = 0; w < (PRIV ? EPI : 1); ++w) {
                     unsigned* sc = scnt + w * SLOTS * nb * 2;
                     c0 += sc[2 * idx];
                     c1 += sc[2 * idx + 1];
@@ -639,7 +649,7 @@ __global__ void __launch_bounds__(128 + 32 * kEpi, 1)
                     if (c1) atomicAdd(&a.r2_counts[(int64_t)blk * nb + bb], c1);
                 }
             }
-            epi_bar<kEpi>();
+            epi_bar<EPI>();
         }
     }
     tc_fence_before();
@@ -691,7 +701,9 @@ size_t smem_bytes_t(int nb, int max_n, int ncopy) {
 
 // Per-warp staging copies when they fit next to the pipeline stages.
 template <int P, bool GENO, int V>
-bool private_staging(int nb, int max_n) { return smem_bytes_t<P, GENO, V>(nb, max_n, kEpi) <= kMaxSmem; }
+bool private_staging(int nb, int max_n) {
+    return smem_bytes_t<P, GENO, V>(nb, max_n, Cfg<P, GENO, V>::EPI) <= kMaxSmem;
+}
 
 template <bool GENO>
 size_t tc_smem_bytes_g(const ParseShape& sh) {
@@ -733,7 +745,7 @@ cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t* o, co
     a.status = w.status;
     // at least half of an SM's shared memory, so that one CTA (holding all 512 TMEM
     // columns) runs per SM
-    size_t smem = smem_bytes_t<P, GENO, V>(d->n_bins, sh.max_n, PRIV ? kEpi : 1);
+    size_t smem = smem_bytes_t<P, GENO, V>(d->n_bins, sh.max_n, PRIV ? C::EPI : 1);
     if (smem < kMinSmem) smem = kMinSmem;
     if (smem > kMaxSmem) return cudaErrorInvalidConfiguration;
     cudaError_t e =
@@ -744,7 +756,7 @@ cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t* o, co
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (n_items == 0) return cudaSuccess;
     const int grid = n_items < sms ? n_items : sms;
-    k_parse_tc<P, T, PRIV, GENO, V><<<grid, 128 + 32 * kEpi, smem, s>>>(mA, mB, a);
+    k_parse_tc<P, T, PRIV, GENO, V><<<grid, 128 + 32 * C::EPI, smem, s>>>(mA, mB, a);
     return cudaGetLastError();
 }
 
