@@ -25,37 +25,46 @@ struct PrepArgs {
     unsigned* status;
 };
 
-constexpr int kPrepV = 64, kPrepK = 128;
+constexpr int kPrepV = 128, kPrepK = 128;
 
 LDK_DEV uint32_t plane_bit(int8_t x, int plane, int genotypes) {
     if (genotypes) return plane == 0 ? (x == 1) : plane == 1 ? (x == 2) : plane == 2 ? (x >= 0 && x <= 2) : 0u;
     return plane == 0 ? (x == 1) : (x == 0 || x == 1);
 }
 
+// One block: 128 K positions (haplotypes / individuals) x 128 SNPs.  The rows of the 128 K
+// positions are resolved once; the gather reads 128-byte row segments of X (consecutive
+// threads, consecutive SNPs) into a shared tile, the scatter writes each SNP's planes as
+// 128-byte runs along K.
 __global__ void __launch_bounds__(256) k_prep_planes(PrepArgs a) {
-    __shared__ int8_t tile[kPrepK][kPrepV + 4];
+    __shared__ int8_t tile[kPrepK][kPrepV + 1];  // odd row length: the scatter's column reads hit distinct banks
+    __shared__ int srow[kPrepK];
     const int64_t v0 = (int64_t)blockIdx.x * kPrepV;
     const int k0 = blockIdx.y * kPrepK;
     const int xmax = a.genotypes ? 2 : 1;
-    // gather: tile[k][v] = X[row(k), v0 + v] (coalesced along v); 127 marks padding
+    for (int kk = threadIdx.x; kk < kPrepK; kk += blockDim.x) {
+        const int k = k0 + kk;
+        int p = 0;
+        while (p + 1 < a.P && k >= a.kofs[p + 1]) ++p;
+        const int local = k - a.kofs[p];
+        const int np = a.pop_off[p + 1] - a.pop_off[p];
+        srow[kk] = (local >= 0 && local < np && k < a.kofs[a.P]) ? a.pop_rows[a.pop_off[p] + local] : -1;
+    }
+    __syncthreads();
+    // gather: tile[k][v] = X[row(k), v0 + v]; 127 marks padding
+    bool bad = false;
     for (int idx = threadIdx.x; idx < kPrepK * kPrepV; idx += blockDim.x) {
         const int kk = idx / kPrepV, vv = idx % kPrepV;
-        const int k = k0 + kk;
         const int64_t v = v0 + vv;
+        const int row = srow[kk];
         int8_t x = 127;
-        if (v < a.n_var) {
-            int p = 0;
-            while (p + 1 < a.P && k >= a.kofs[p + 1]) ++p;
-            const int local = k - a.kofs[p];
-            const int np = a.pop_off[p + 1] - a.pop_off[p];
-            if (local >= 0 && local < np && k < a.kofs[a.P]) {
-                const int row = a.pop_rows[a.pop_off[p] + local];
-                x = a.X[(int64_t)row * a.ld + v];
-                if (x < -1 || x > xmax) atomicOr(a.status, LDK_DEVERR_BAD_INPUT);
-            }
+        if (row >= 0 && v < a.n_var) {
+            x = __ldg(a.X + (int64_t)row * a.ld + v);
+            bad |= (x < -1 || x > xmax);
         }
         tile[kk][vv] = x;
     }
+    if (bad) atomicOr(a.status, LDK_DEVERR_BAD_INPUT);
     __syncthreads();
     // scatter: 4 bytes of one plane per thread, coalesced along k
     for (int idx = threadIdx.x; idx < kPrepV * a.planes * (kPrepK / 4); idx += blockDim.x) {
