@@ -43,10 +43,15 @@ namespace ldk {
 namespace {
 
 constexpr int kKChunk = 128;            // K bytes per TMA box / swizzle row
-constexpr int kEpi = 4;                 // epilogue warps, one per TMEM lane quarter
 constexpr int kRing = 2;                // claimed row blocks in flight between the roles
 constexpr int kTmemCols = 512;
 constexpr uint64_t kTimeoutNs = 5000000000ull;  // 5 s per wait
+// Register split of the SPLIT layout (384 threads): the launch gives every thread
+// kRegLaunch registers; warpgroup 0 drops to kRegCtrl and the two epilogue warpgroups rise
+// to kRegEpi, which the freed registers cover exactly.  Both return to kRegLaunch before
+// the teardown, and the host launches only a kernel compiled to kRegLaunch registers.
+constexpr int kRegLaunch = 168, kRegCtrl = 24, kRegEpi = 240;
+static_assert(4 * kRegCtrl + 8 * kRegEpi == 12 * kRegLaunch, "register split must use the launch allocation");
 constexpr size_t kMinSmem = 116 * 1024;
 constexpr size_t kMaxSmem = 227 * 1024;
 
@@ -80,9 +85,23 @@ struct Cfg {
     static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
     static constexpr int NS = HapNStats<P>::value;
     static constexpr int SLOTS = GENO ? 4 : 2;                         // bootstrap blocks staged per row block
-    // epilogue warps: one per TMEM lane quarter, or -- for one population, whose epilogue
-    // needs few registers -- two, each taking half of every partner tile
-    static constexpr int EPI = P == 1 ? 8 : 4;
+    // Warp layout.  Warp w may read only TMEM lane quarter w % 4, and each of the four
+    // schedulers of an SM holds warps w, w + 4, ... with a quarter of the register file.
+    //  * SPLIT (haplotypes, three or four populations, whose estimators need ~240
+    //    registers): 12 warps.  Warpgroup 0 (TMA, MMA, two idle warps) gives its registers
+    //    up with setmaxnreg (kRegCtrl each) and the eight epilogue warps 4..11, two per
+    //    lane quarter, take them (kRegEpi each), so that every scheduler holds two
+    //    full-register epilogue warps beside one control warp.
+    //  * EPI == 8 otherwise (one population; two haplotype populations): warps 0 and 1
+    //    issue TMA and MMA, warps 2..9 are the epilogue (≤ 168 registers, since two
+    //    schedulers hold three warps).
+    //  * EPI == 4 (genotypes, two or more populations): warps 0, 1 TMA and MMA, 2 and 3
+    //    idle, 4..7 one epilogue warp per lane quarter (255 registers).
+    // With two epilogue warps per lane quarter each takes half of every partner tile.
+    static constexpr bool SPLIT = !GENO && P >= 3;
+    static constexpr int EPI = (SPLIT || P == 1 || (!GENO && P == 2)) ? 8 : 4;
+    static constexpr int W0 = (EPI == 8 && !SPLIT) ? 2 : 4;  // first epilogue warp
+    static constexpr int THREADS = 32 * (W0 + EPI);
     static_assert(NBUF * COLS <= kTmemCols, "TMEM budget");
     static_assert(N % 16 == 0 && N <= 256, "MMA N");
 };
@@ -208,6 +227,12 @@ LDK_DEV bool epi_bar_or(bool pred) {
     return r != 0;
 }
 
+// Warpgroup-wide register budget changes (all four warps of the warpgroup execute them).
+template <int N>
+LDK_DEV void setmaxnreg_inc() { asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(N)); }
+template <int N>
+LDK_DEV void setmaxnreg_dec() { asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(N)); }
+
 LDK_DEV void spin_ns(uint64_t ns) {
     const uint64_t t0 = global_ns();
     while (global_ns() - t0 < ns) {
@@ -250,45 +275,73 @@ struct Pipe {
     volatile int* abort_s;
 };
 
+// Partner tiles of row block `item` (rows [row0, row1), partners up to jmax[row1 - 1]).
+template <class C>
+LDK_DEV int tile_count(const TcArgs& a, int item, int& row0) {
+    row0 = a.items[2 * item];
+    const int row1 = a.items[2 * item + 1];
+    const int jend = a.jmax[row1 - 1];
+    return jend > row0 + 1 ? (jend - row0 + C::NJ - 1) / C::NJ : 0;
+}
+
+// TMA loads of K chunk c of the tile (row block at row0, partners from j0) into stage s.
+template <class C>
+LDK_DEV void issue_loads(const Pipe& S, const CUtensorMap* tmA, const CUtensorMap* tmB, int s, int c, int row0,
+                         int j0) {
+    unsigned char* dst = S.stages + s * C::STAGE_BYTES;
+    mbar_expect_tx(&S.full_bar[s], C::STAGE_BYTES);
+#pragma unroll
+    for (int x = 0; x < C::REGIONS; ++x) tma_load_3d(dst + x * C::A_BOX, tmA, &S.full_bar[s], c * kKChunk, x, row0);
+    tma_load_3d(dst + C::A_BYTES, tmB, &S.full_bar[s], c * kKChunk, 0, j0);
+}
+
+// MMAs of K chunk c (in stage s) into accumulator buffer buf; frees the stage on completion.
+template <class C, int P>
+LDK_DEV void issue_mmas(const Pipe& S, uint32_t tmem, const TcArgs& a, int s, int c, uint32_t buf) {
+    constexpr uint32_t idesc = idesc_u8<C::N>();
+    const uint32_t a_addr = su32(S.stages + s * C::STAGE_BYTES);
+    const uint32_t b_addr = a_addr + C::A_BYTES;
+#pragma unroll
+    for (int ks = 0; ks < kKChunk / 32; ++ks) {
+        const int kbyte = c * kKChunk + ks * 32;
+        int p = 0;
+#pragma unroll
+        for (int q = 1; q < P; ++q) p += (kbyte >= a.kofs[q]) ? 1 : 0;
+        const uint32_t first = (kbyte == a.kofs[p]) ? 1u : 0u;
+#pragma unroll
+        for (int x = 0; x < C::REGIONS; ++x) {
+            const uint32_t d = tmem + buf * C::COLS + (p * C::REGIONS + x) * C::N;
+            mma_u8(d, sw128_desc(a_addr + x * C::A_BOX + ks * 32), sw128_desc(b_addr + ks * 32), idesc, first ^ 1u);
+        }
+    }
+    mma_commit(&S.empty_bar[s]);
+}
+
 // Warp 0: claims row blocks from the global counter, publishes them through the ring and
 // issues the TMA loads of every partner tile's K chunks.
 template <class C>
 LDK_DEV void run_producer(const Pipe& S, const CUtensorMap* tmA, const CUtensorMap* tmB, const TcArgs& a,
                           int lane) {
-    unsigned char* stages = S.stages;
-    uint64_t* full_bar = S.full_bar;
-    uint64_t* empty_bar = S.empty_bar;
-    uint64_t* ifull = S.ifull;
-    uint64_t* iempty = S.iempty;
-    volatile int* ring = S.ring;
-    volatile int* abort_s = S.abort_s;
     if (lane == 0) {
         uint32_t it = 0;
         bool ok = true;
         for (uint32_t k = 0; ok; ++k) {
             // claim the next row block and publish it to the MMA issuer and the epilogue
             const int sl = k % kRing;
-            if (!mbar_wait(&iempty[sl], ((k / kRing) & 1u) ^ 1u, abort_s, a.status)) { ok = false; break; }
+            if (!mbar_wait(&S.iempty[sl], ((k / kRing) & 1u) ^ 1u, S.abort_s, a.status)) { ok = false; break; }
             int item = atomicAdd(a.item_counter, 1);
             if (item >= a.n_items) item = -1;
-            ring[sl] = item;
-            mbar_arrive(&ifull[sl]);
+            S.ring[sl] = item;
+            mbar_arrive(&S.ifull[sl]);
             if (item < 0) break;
-            const int row0 = a.items[2 * item], row1 = a.items[2 * item + 1];
-            const int jend = a.jmax[row1 - 1];
-            const int n_jt = jend > row0 + 1 ? (jend - row0 + C::NJ - 1) / C::NJ : 0;
+            int row0;
+            const int n_jt = tile_count<C>(a, item, row0);
             for (int t = 0; t < n_jt && ok; ++t) {
-                const int j0 = row0 + t * C::NJ;
                 for (int c = 0; c < a.nkc; ++c, ++it) {
                     const int s = it % C::STAGES;
                     const uint32_t ph = (it / C::STAGES) & 1u;
-                    if (!mbar_wait(&empty_bar[s], ph ^ 1u, abort_s, a.status)) { ok = false; break; }
-                    unsigned char* dst = stages + s * C::STAGE_BYTES;
-                    mbar_expect_tx(&full_bar[s], C::STAGE_BYTES);
-#pragma unroll
-                    for (int x = 0; x < C::REGIONS; ++x)
-                        tma_load_3d(dst + x * C::A_BOX, tmA, &full_bar[s], c * kKChunk, x, row0);
-                    tma_load_3d(dst + C::A_BYTES, tmB, &full_bar[s], c * kKChunk, 0, j0);
+                    if (!mbar_wait(&S.empty_bar[s], ph ^ 1u, S.abort_s, a.status)) { ok = false; break; }
+                    issue_loads<C>(S, tmA, tmB, s, c, row0, row0 + t * C::NJ);
                 }
             }
         }
@@ -300,57 +353,30 @@ LDK_DEV void run_producer(const Pipe& S, const CUtensorMap* tmA, const CUtensorM
 // Warp 1: one thread issues the MMAs of every tile into the double-buffered accumulators.
 template <class C, int P>
 LDK_DEV void run_mma(const Pipe& S, uint32_t tmem, const TcArgs& a, int lane) {
-    unsigned char* stages = S.stages;
-    uint64_t* full_bar = S.full_bar;
-    uint64_t* empty_bar = S.empty_bar;
-    uint64_t* tfull = S.tfull;
-    uint64_t* tempty = S.tempty;
-    uint64_t* ifull = S.ifull;
-    uint64_t* iempty = S.iempty;
-    volatile int* ring = S.ring;
-    volatile int* abort_s = S.abort_s;
     if (lane == 0) {
-        constexpr uint32_t idesc = idesc_u8<C::N>();
         uint32_t it = 0, tcount = 0;
         bool ok = true;
         for (uint32_t k = 0; ok; ++k) {
             const int sl = k % kRing;
-            if (!mbar_wait(&ifull[sl], (k / kRing) & 1u, abort_s, a.status)) { ok = false; break; }
-            const int item = ring[sl];
-            mbar_arrive(&iempty[sl]);
+            if (!mbar_wait(&S.ifull[sl], (k / kRing) & 1u, S.abort_s, a.status)) { ok = false; break; }
+            const int item = S.ring[sl];
+            mbar_arrive(&S.iempty[sl]);
             if (item < 0) break;
-            const int row0 = a.items[2 * item], row1 = a.items[2 * item + 1];
-            const int jend = a.jmax[row1 - 1];
-            const int n_jt = jend > row0 + 1 ? (jend - row0 + C::NJ - 1) / C::NJ : 0;
+            int row0;
+            const int n_jt = tile_count<C>(a, item, row0);
             for (int t = 0; t < n_jt && ok; ++t, ++tcount) {
                 const uint32_t buf = tcount % C::NBUF, tph = (tcount / C::NBUF) & 1u;
-                if (!mbar_wait(&tempty[buf], tph ^ 1u, abort_s, a.status)) { ok = false; break; }
+                if (!mbar_wait(&S.tempty[buf], tph ^ 1u, S.abort_s, a.status)) { ok = false; break; }
                 tc_fence_after();
                 for (int c = 0; c < a.nkc; ++c, ++it) {
                     const int s = it % C::STAGES;
                     const uint32_t ph = (it / C::STAGES) & 1u;
-                    if (!mbar_wait(&full_bar[s], ph, abort_s, a.status)) { ok = false; break; }
+                    if (!mbar_wait(&S.full_bar[s], ph, S.abort_s, a.status)) { ok = false; break; }
                     tc_fence_after();
-                    const uint32_t a_addr = su32(stages + s * C::STAGE_BYTES);
-                    const uint32_t b_addr = a_addr + C::A_BYTES;
-#pragma unroll
-                    for (int ks = 0; ks < kKChunk / 32; ++ks) {
-                        const int kbyte = c * kKChunk + ks * 32;
-                        int p = 0;
-#pragma unroll
-                        for (int q = 1; q < P; ++q) p += (kbyte >= a.kofs[q]) ? 1 : 0;
-                        const uint32_t first = (kbyte == a.kofs[p]) ? 1u : 0u;
-#pragma unroll
-                        for (int x = 0; x < C::REGIONS; ++x) {
-                            const uint32_t d = tmem + buf * C::COLS + (p * C::REGIONS + x) * C::N;
-                            mma_u8(d, sw128_desc(a_addr + x * C::A_BOX + ks * 32), sw128_desc(b_addr + ks * 32),
-                                   idesc, first ^ 1u);
-                        }
-                    }
-                    mma_commit(&empty_bar[s]);
+                    issue_mmas<C, P>(S, tmem, a, s, c, buf);
                 }
                 if (!ok) break;
-                mma_commit(&tfull[buf]);
+                mma_commit(&S.tfull[buf]);
             }
         }
         if (!ok) spin_ns(2000000);
@@ -359,7 +385,7 @@ LDK_DEV void run_mma(const Pipe& S, uint32_t tmem, const TcArgs& a, int lane) {
 }
 
 template <int P, typename T, bool PRIV, bool GENO, int V>
-__global__ void __launch_bounds__(128 + 32 * Cfg<P, GENO, V>::EPI, 1)
+__global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
     k_parse_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcArgs a) {
     using C = Cfg<P, GENO, V>;
     constexpr int NS = C::NS;
@@ -412,11 +438,17 @@ __global__ void __launch_bounds__(128 + 32 * Cfg<P, GENO, V>::EPI, 1)
     tc_fence_after();
     const uint32_t tmem = tmem_base_s;
     const Pipe pipe{stages, full_bar, empty_bar, tfull, tempty, ifull, iempty, ring, &abort_s};
-    if (warp == 0) run_producer<C>(pipe, &tmA, &tmB, a, lane);
-    else if (warp == 1) run_mma<C, P>(pipe, tmem, a, lane);
-    if (warp >= 4) {
+    // Each side keeps its setmaxnreg region to itself and returns to the launch count
+    // before the teardown, so that no code is reachable under two register budgets.
+    if (warp < C::W0) {
+        if constexpr (C::SPLIT) setmaxnreg_dec<kRegCtrl>();
+        if (warp == 0) run_producer<C>(pipe, &tmA, &tmB, a, lane);
+        else if (warp == 1) run_mma<C, P>(pipe, tmem, a, lane);
+        if constexpr (C::SPLIT) setmaxnreg_inc<kRegLaunch>();
+    } else {
+        if constexpr (C::SPLIT) setmaxnreg_inc<kRegEpi>();
         // ------------------------------------------------------------- epilogue
-        const int e = warp - 4;
+        const int e = warp - C::W0;
         const int L = (warp & 3) * 32 + lane;
         // haplotype rows: lanes 2r, 2r+1 share SNP r and split its partners by parity;
         // genotype rows: lane L is SNP L and takes every partner.  With two warps per lane
@@ -616,7 +648,7 @@ __global__ void __launch_bounds__(128 + 32 * Cfg<P, GENO, V>::EPI, 1)
             (void)ok;
             // staging -> global, once per row block
             epi_bar<EPI>();
-            const int et = threadIdx.x - 128;
+            const int et = threadIdx.x - 32 * C::W0;
             for (int idx = et; idx < stage_n; idx += 32 * EPI) {
                 double val = 0.0;
 #pragma unroll
@@ -651,6 +683,7 @@ __global__ void __launch_bounds__(128 + 32 * Cfg<P, GENO, V>::EPI, 1)
             }
             epi_bar<EPI>();
         }
+        if constexpr (C::SPLIT) setmaxnreg_dec<kRegLaunch>();
     }
     tc_fence_before();
     __syncthreads();
@@ -751,12 +784,20 @@ cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t* o, co
     cudaError_t e =
         cudaFuncSetAttribute(k_parse_tc<P, T, PRIV, GENO, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    if constexpr (C::SPLIT) {
+        // the register split adds up only at kRegLaunch registers per thread; any other
+        // allocation would leave setmaxnreg.inc waiting, so such a build is not launched
+        cudaFuncAttributes fa;
+        e = cudaFuncGetAttributes(&fa, k_parse_tc<P, T, PRIV, GENO, V>);
+        if (e != cudaSuccess) return e;
+        if (fa.numRegs != kRegLaunch) return cudaErrorInvalidKernelImage;
+    }
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (n_items == 0) return cudaSuccess;
     const int grid = n_items < sms ? n_items : sms;
-    k_parse_tc<P, T, PRIV, GENO, V><<<grid, 128 + 32 * C::EPI, smem, s>>>(mA, mB, a);
+    k_parse_tc<P, T, PRIV, GENO, V><<<grid, C::THREADS, smem, s>>>(mA, mB, a);
     return cudaGetLastError();
 }
 
