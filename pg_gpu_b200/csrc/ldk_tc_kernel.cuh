@@ -48,8 +48,8 @@ constexpr int kTmemCols = 512;
 constexpr uint64_t kTimeoutNs = 5000000000ull;  // 5 s per wait
 // Register split of the SPLIT layout (384 threads): the launch gives every thread
 // kRegLaunch registers; warpgroup 0 drops to kRegCtrl and the two epilogue warpgroups rise
-// to kRegEpi, which the freed registers cover exactly.  Both return to kRegLaunch before
-// the teardown, and the host launches only a kernel compiled to kRegLaunch registers.
+// to kRegEpi, which the freed registers cover exactly.  The host launches only a kernel
+// compiled to kRegLaunch registers.
 constexpr int kRegLaunch = 168, kRegCtrl = 24, kRegEpi = 240;
 static_assert(4 * kRegCtrl + 8 * kRegEpi == 12 * kRegLaunch, "register split must use the launch allocation");
 constexpr size_t kMinSmem = 116 * 1024;
@@ -438,13 +438,17 @@ __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
     tc_fence_after();
     const uint32_t tmem = tmem_base_s;
     const Pipe pipe{stages, full_bar, empty_bar, tfull, tempty, ifull, iempty, ring, &abort_s};
-    // Each side keeps its setmaxnreg region to itself and returns to the launch count
-    // before the teardown, so that no code is reachable under two register budgets.
+    // Each side changes its register budget once, at its start, and never back: warpgroup
+    // 0 releases registers (setmaxnreg.dec never waits) and the epilogue warps take them
+    // (setmaxnreg.inc waits only for that release, which comes unconditionally first).
+    // No later increase exists that could wait on registers another warp holds -- a
+    // restore to the launch count by warpgroup 0, whose idle warps would reach it at once,
+    // could take the registers back before the epilogue's increase and starve it.  The
+    // code both sides share, the teardown below, fits the smaller budget.
     if (warp < C::W0) {
         if constexpr (C::SPLIT) setmaxnreg_dec<kRegCtrl>();
         if (warp == 0) run_producer<C>(pipe, &tmA, &tmB, a, lane);
         else if (warp == 1) run_mma<C, P>(pipe, tmem, a, lane);
-        if constexpr (C::SPLIT) setmaxnreg_inc<kRegLaunch>();
     } else {
         if constexpr (C::SPLIT) setmaxnreg_inc<kRegEpi>();
         // ------------------------------------------------------------- epilogue
@@ -683,7 +687,6 @@ __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
             }
             epi_bar<EPI>();
         }
-        if constexpr (C::SPLIT) setmaxnreg_dec<kRegLaunch>();
     }
     tc_fence_before();
     __syncthreads();
