@@ -87,20 +87,18 @@ struct Cfg {
     static constexpr int SLOTS = GENO ? 4 : 2;                         // bootstrap blocks staged per row block
     // Warp layout.  Warp w may read only TMEM lane quarter w % 4, and each of the four
     // schedulers of an SM holds warps w, w + 4, ... with a quarter of the register file.
-    //  * SPLIT (haplotypes, three or four populations, whose estimators need ~240
-    //    registers): 12 warps.  Warpgroup 0 (TMA, MMA, two idle warps) gives its registers
-    //    up with setmaxnreg (kRegCtrl each) and the eight epilogue warps 4..11, two per
-    //    lane quarter, take them (kRegEpi each), so that every scheduler holds two
-    //    full-register epilogue warps beside one control warp.
-    //  * EPI == 8 otherwise (one population; two haplotype populations): warps 0 and 1
-    //    issue TMA and MMA, warps 2..9 are the epilogue (≤ 168 registers, since two
+    // Eight epilogue warps, two per lane quarter, each take half of every partner tile.
+    //  * SPLIT (genotypes; haplotypes with three or four populations -- estimators that
+    //    want ~240 registers): 12 warps.  Warpgroup 0 (TMA, MMA, two idle warps) gives its
+    //    registers up with setmaxnreg (kRegCtrl each) and the epilogue warps 4..11 take
+    //    them (kRegEpi each), so that every scheduler holds two full-register epilogue
+    //    warps beside one control warp.
+    //  * otherwise (one or two haplotype populations, ≤ 160 registers): 10 warps, TMA and
+    //    MMA in warps 0 and 1, the epilogue in warps 2..9 (168 registers at most, since two
     //    schedulers hold three warps).
-    //  * EPI == 4 (genotypes, two or more populations): warps 0, 1 TMA and MMA, 2 and 3
-    //    idle, 4..7 one epilogue warp per lane quarter (255 registers).
-    // With two epilogue warps per lane quarter each takes half of every partner tile.
-    static constexpr bool SPLIT = !GENO && P >= 3;
-    static constexpr int EPI = (SPLIT || P == 1 || (!GENO && P == 2)) ? 8 : 4;
-    static constexpr int W0 = (EPI == 8 && !SPLIT) ? 2 : 4;  // first epilogue warp
+    static constexpr bool SPLIT = GENO || P >= 3;
+    static constexpr int EPI = 8;
+    static constexpr int W0 = SPLIT ? 4 : 2;  // first epilogue warp
     static constexpr int THREADS = 32 * (W0 + EPI);
     static_assert(NBUF * COLS <= kTmemCols, "TMEM budget");
     static_assert(N % 16 == 0 && N <= 256, "MMA N");
