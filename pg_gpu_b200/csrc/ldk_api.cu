@@ -316,8 +316,11 @@ int enqueue_device(const ldk_parse_t* d, const ldk_parse_out_t* out, const Prepa
         if (prof) cudaEventRecord(g_ev[1], s);
     } else {
         if ((rc = check_cuda(launch_prep_planes(&dd, P.w, P.sh, s), "indicator planes"))) return rc;
-        if (tune && n_variants(d, P.sh) > 1 && tuned_variant(d, P.sh) < 0)
+        if (tune && n_variants(d, P.sh) > 1 && tuned_variant(d, P.sh) < 0) {
             if ((rc = autotune_tc(&dd, out, P, s))) return rc;
+            // the candidate runs left their sums and a spent row-block counter behind
+            if ((rc = clear(&dd, out, P, s))) return rc;
+        }
         const int v = tuned_variant(d, P.sh);
         if (prof) cudaEventRecord(g_ev[0], s);
         if ((rc = check_cuda(launch_parse_tc(&dd, out, P.w, P.sh, P.L.n_items, v < 0 ? 0 : v, s), "tensor-core parse")))

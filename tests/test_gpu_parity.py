@@ -367,8 +367,9 @@ def test_parse_graph_replay_matches_run(method):
 @pytest.mark.parametrize("genotypes", [False, True])
 def test_autotune_picks_a_candidate_and_keeps_results(genotypes):
     """With tuning on, the first parse of a shape times the tile candidates and keeps one;
-    its results and those of later calls (tuned width) match the default-width parse."""
-    w = synth.make_config(3 if genotypes else 2, scale=0.01)
+    its results and those of later calls (tuned width) match the default-width parse, and
+    the first call's own parse (after the candidates) does the full work again."""
+    w = synth.make_config(3 if genotypes else 2, scale=0.1)
     kw = dict(genotypes=w.genotypes, method="tc", max_dist=w.max_dist, window_offsets=w.window_offsets,
               snp_block=w.snp_block, n_blocks=w.n_blocks)
     ref = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, **kw)
@@ -376,10 +377,17 @@ def test_autotune_picks_a_candidate_and_keeps_results(genotypes):
     try:
         _lib.autotune(True)
         p = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, **kw)
+        lib = _lib.load()
+        lib.ldk_profile(1)
+        kernel_ms = []
         for _ in range(2):
             got = p.run().numpy()
+            kernel_ms.append(lib.ldk_profile_last_kernel_ms())
             np.testing.assert_array_equal(got["pairs"], want["pairs"])
             assert rel_err(got["sums"], want["sums"], 1e-300) < 1e-11
         assert p.tile_width() in ({16, 8} if genotypes else {64, 32})
+        # a parse launched on the candidates' spent row-block counter would finish at once
+        assert kernel_ms[0] > 0.3 * kernel_ms[1], kernel_ms
     finally:
+        _lib.load().ldk_profile(0)
         _lib.autotune(False)
