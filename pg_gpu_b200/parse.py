@@ -6,7 +6,11 @@ float64 sums of the moments-ordered statistics, pair counts, and the sum and cou
 finite r^2.  Two counting/estimator methods:
 
 * ``"plain"`` -- per-pair byte counting + FP64 estimators (the reference's design);
-* ``"tc"``    -- INT8 tcgen05 Gram-product counts + FP32 estimators, FP64 bin sums.
+* ``"tc"``    -- INT8 tcgen05 Gram-product counts + FP64 estimators and bin sums;
+* ``"tc32"``  -- the same counts with FP32 estimators (FP64 bin sums).
+
+``Pipeline`` runs a stream of same-shape parses from pinned host memory with the copies
+overlapped with the parses.
 """
 from __future__ import annotations
 
@@ -179,6 +183,83 @@ class Parser:
             out = self.enqueue()
             extra = after(out) if after is not None else None
         return g, extra
+
+
+class Pipeline:
+    """A stream of same-shape parses fed from pinned host memory, with the host-to-device
+    copy of each batch and the device-to-host copy of each result overlapped with the
+    parses of the neighbouring batches.
+
+    ``make_slot()`` builds one slot and returns ``(parser, inputs, after)``: a ``Parser``;
+    a dict naming the device tensors a step reads (the parser's ``X``, ``pos``, ``block``
+    and any tensor ``after`` reads), which ``submit`` fills from host tensors of the same
+    names; and ``after(out)``, torch work on the parse outputs captured into the slot's
+    CUDA graph (e.g. bootstrap replicates via ``block_combine``), returning a tuple of
+    device tensors, or None.  Every slot has its own inputs, workspace, outputs and graph,
+    so batch k + 1 is copied in while batch k is parsed and batch k - 1 copied out (three
+    streams ordered by events).
+
+    ``submit(host_inputs, host_outputs)`` enqueues one batch: ``host_outputs`` receives
+    ``(sums, pairs, *after(...))`` of that batch, each a pinned host tensor of the matching
+    shape; they are valid after ``drain()``.  The caller must not reuse a batch's host
+    tensors before then (or before the batch ``slots`` places later has been submitted
+    and drained)."""
+
+    def __init__(self, make_slot, slots: int = 2):
+        torch = _lib.require_cuda()
+        self.torch = torch
+        if slots < 1:
+            raise ValueError("slots must be >= 1")
+        self.slots = []
+        for _ in range(slots):
+            parser, inputs, after = make_slot()
+            graph, extra = parser.graph(after=after)
+            extra = () if extra is None else tuple(extra)
+            self.slots.append((parser, dict(inputs), graph, (parser.out.sums, parser.out.pairs) + extra))
+        self.h2d, self.compute, self.d2h = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+        self.ready = [torch.cuda.Event() for _ in range(slots)]
+        self.parsed = [torch.cuda.Event() for _ in range(slots)]
+        self.free = [torch.cuda.Event() for _ in range(slots)]
+        self.k = 0
+
+    def submit(self, host_inputs: dict, host_outputs) -> None:
+        torch = self.torch
+        s = self.k % len(self.slots)
+        parser, inputs, graph, outs = self.slots[s]
+        caller = torch.cuda.current_stream()
+        if set(host_inputs) != set(k for k, v in inputs.items() if v is not None):
+            raise KeyError(f"host inputs {sorted(host_inputs)} do not match the slot's {sorted(inputs)}")
+        if len(host_outputs) != len(outs):
+            raise ValueError(f"{len(outs)} host outputs expected")
+        for st in (self.h2d, self.compute, self.d2h):
+            st.wait_stream(caller)  # work the caller enqueued first (e.g. a start event)
+        with torch.cuda.stream(self.h2d):
+            self.h2d.wait_event(self.free[s])  # the slot's previous batch is parsed and copied out
+            for name, h in host_inputs.items():
+                inputs[name].copy_(h, non_blocking=True)
+            self.ready[s].record(self.h2d)
+        with torch.cuda.stream(self.compute):
+            self.compute.wait_event(self.ready[s])
+            graph.replay()
+            self.parsed[s].record(self.compute)
+        with torch.cuda.stream(self.d2h):
+            self.d2h.wait_event(self.parsed[s])
+            for h, d in zip(host_outputs, outs):
+                h.copy_(d, non_blocking=True)
+            self.free[s].record(self.d2h)
+        self.k += 1
+
+    def drain(self) -> None:
+        """Make the caller's stream wait for every submitted batch; the host outputs are
+        valid once that stream is synchronised (``status()`` checks the device status)."""
+        caller = self.torch.cuda.current_stream()
+        for st in (self.h2d, self.compute, self.d2h):
+            caller.wait_stream(st)
+
+    def status(self) -> None:
+        """Synchronise and raise LdkError if a slot's last parse set a device error."""
+        for parser, _, _, _ in self.slots:
+            parser.status()
 
 
 def ld_parse(data, positions, pop_rows, edges, **kw) -> ParseResult:

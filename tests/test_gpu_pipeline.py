@@ -1,0 +1,78 @@
+"""parse.Pipeline: a stream of same-shape batches from pinned host memory, double-buffered.
+Each batch's results, copied back through the pipeline, must equal a resident Parser run on
+the same input: pair tallies bit-exact, sums to 1e-12 (FP64 sums in another order)."""
+import numpy as np
+import pytest
+
+from pg_gpu_b200 import parse, synth
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _batches(w, n, seed):
+    """n haplotype matrices of the workload's shape: alleles flipped at random (missing
+    calls kept), so every batch has different counts."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        x = w.data.copy()
+        flip = (rng.random(x.shape) < 0.1) & (x >= 0)
+        x[flip] = 1 - x[flip]
+        out.append(x)
+    return out
+
+
+@pytest.mark.parametrize("slots", [1, 2])
+def test_pipeline_matches_resident_parses(slots):
+    w = synth.make_config(4, scale=0.004)
+    kw = dict(genotypes=w.genotypes, method="tc", max_dist=w.max_dist, window_offsets=w.window_offsets,
+              snp_block=w.snp_block, n_blocks=w.n_blocks)
+    reps_w = torch.as_tensor(w.replicate_weights, dtype=torch.int32, device="cuda")
+
+    def make_slot():
+        p = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, **kw)
+        rw = reps_w.clone()
+        return p, {"X": p.X, "pos": p.pos, "block": p.block, "reps_w": rw}, \
+            (lambda out: (parse.block_combine(out.sums, rw),))
+
+    pipe = parse.Pipeline(make_slot, slots=slots)
+    batches = _batches(w, 3, seed=11)
+    pos_h = torch.from_numpy(w.positions.copy()).pin_memory()
+    blk_h = torch.from_numpy(w.snp_block.copy()).pin_memory()
+    rw_h = reps_w.cpu().pin_memory()
+    ref = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, **kw)
+    sums_shape, pairs_shape = tuple(ref.out.sums.shape), tuple(ref.out.pairs.shape)
+    rep_shape = (reps_w.shape[0],) + sums_shape[1:]
+    outs = [[torch.empty(sums_shape, dtype=torch.float64).pin_memory(),
+             torch.empty(pairs_shape, dtype=torch.int64).pin_memory(),
+             torch.empty(rep_shape, dtype=torch.float64).pin_memory()] for _ in batches]
+    for b, o in zip(batches, outs):
+        pipe.submit({"X": torch.from_numpy(b).pin_memory(), "pos": pos_h, "block": blk_h, "reps_w": rw_h}, o)
+    pipe.drain()
+    torch.cuda.synchronize()
+    pipe.status()
+    for b, o in zip(batches, outs):
+        r = parse.Parser(b, w.positions, w.pop_rows, w.edges, **kw).run()
+        want_sums = r.sums.cpu().numpy()
+        np.testing.assert_array_equal(o[1].numpy(), r.pairs.cpu().numpy())
+        np.testing.assert_allclose(o[0].numpy(), want_sums, rtol=1e-12, atol=1e-300)
+        want_reps = parse.block_combine(r.sums, reps_w).cpu().numpy()
+        np.testing.assert_allclose(o[2].numpy(), want_reps, rtol=1e-12, atol=1e-300)
+    # the batches differ, so a slot that kept an earlier batch's inputs would have failed
+    assert not np.array_equal(outs[0][0].numpy(), outs[1][0].numpy())
+
+
+def test_pipeline_rejects_mismatched_inputs():
+    w = synth.make_config(2, scale=0.004)
+
+    def make_slot():
+        p = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, method="tc", max_dist=w.max_dist)
+        return p, {"X": p.X, "pos": p.pos}, None
+
+    pipe = parse.Pipeline(make_slot, slots=2)
+    with pytest.raises(KeyError):
+        pipe.submit({"X": torch.from_numpy(w.data).pin_memory()}, [None, None])
+    with pytest.raises(ValueError):
+        pipe.submit({"X": torch.from_numpy(w.data).pin_memory(),
+                     "pos": torch.from_numpy(w.positions).pin_memory()}, [None])
