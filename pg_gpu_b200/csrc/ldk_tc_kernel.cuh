@@ -442,7 +442,10 @@ __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
     // No later increase exists that could wait on registers another warp holds -- a
     // restore to the launch count by warpgroup 0, whose idle warps would reach it at once,
     // could take the registers back before the epilogue's increase and starve it.  The
-    // code both sides share, the teardown below, fits the smaller budget.
+    // code both sides share, the teardown below, fits the smaller budget.  Neither the
+    // roles nor the teardown may call a function (printf, a non-inlined helper): a
+    // callee's registers are not bounded by the budget, and a call from a warp holding
+    // kRegCtrl registers raised an illegal-instruction fault.
     if (warp < C::W0) {
         if constexpr (C::SPLIT) setmaxnreg_dec<kRegCtrl>();
         if (warp == 0) run_producer<C>(pipe, &tmA, &tmB, a, lane);
