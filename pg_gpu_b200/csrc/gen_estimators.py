@@ -23,6 +23,7 @@ Run ``python -m pg_gpu_b200.csrc.gen_estimators`` to regenerate; ``build()`` doe
 """
 from __future__ import annotations
 
+import functools
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -495,6 +496,54 @@ GENO_FEATURES = [
 ]
 
 
+# The three single-population polynomials, as pg_gpu writes them, are sums of up to 155
+# integer-coefficient monomials of degree <= 3 in the nine cell counts (~950 FP64 instructions
+# per population and pair with a*b + c fused).  The generated code evaluates them in
+# multivariate Horner form over g1, ..., g9 instead (~400): with integer counts every
+# intermediate of either form is an integer, so FP64 gives the same value exactly while the
+# intermediates stay below 2^53 (more than 10^4 individuals per population before that can
+# fail; the expanded form has the same limit).  check() proves each Horner form equal to its
+# polynomial.
+_HORNER_POLYS = {"GENO_DD_POLY": GENO_DD_POLY, "GENO_DZ_QUARTIC": GENO_DZ_QUARTIC, "GENO_PI2_CORR": GENO_PI2_CORR}
+
+
+def _horner_sympy(poly):
+    import sympy as sp
+    from sympy.polys.polyfuncs import horner
+    g = sp.symbols("g1:10")
+    loc = {f"g{i + 1}": g[i] for i in range(9)}
+    e = sp.expand(sp.sympify(poly.replace("x.g", "g"), locals=loc))
+    return e, horner(e, *g), g
+
+
+@functools.lru_cache(maxsize=None)
+def horner_form(poly):
+    """``poly`` (a polynomial string in x.g1 .. x.g9) in multivariate Horner form, as an
+    expression string in the same variables (C and Python syntax)."""
+    import re
+    _, h, _ = _horner_sympy(poly)
+    out = re.sub(r"\bg(\d)\b", r"x.g\1", str(h))
+    if "**" in out:
+        raise ValueError("power left in a Horner form")
+    return out
+
+
+@functools.lru_cache(maxsize=None)
+def geno_features():
+    """GENO_FEATURES with the three single-population polynomials in Horner form (the form
+    the generated code and the NumPy evaluation use)."""
+    out = []
+    for n, e in GENO_FEATURES:
+        for poly in _HORNER_POLYS.values():
+            e = e.replace("(" + poly + ")", "(" + horner_form(poly) + ")")
+        out.append((n, e))
+    for n in ("DD1", "DZ1", "PI1"):
+        e = dict(out)[n]
+        if any(poly in e for poly in _HORNER_POLYS.values()):
+            raise ValueError(f"{n}: polynomial not replaced")
+    return out
+
+
 def geno_call_expr(case, args):
     """Expression of one canonical raw genotype call (genotype_kernels.py:27-405)."""
     f = lambda p, name: f"f[{p}].{name}"  # noqa: E731
@@ -598,7 +647,7 @@ def emit_geno(P):
     L = [f"// genotype path, P = {P}: {len(stats)} statistics from {len(calls)} distinct raw calls",
          "template <typename T>", f"LDK_DEV void geno_features_P{P}(GenoFeat<T>& x) {{",
          "    geno_prepare(x);"]
-    for n, e in GENO_FEATURES:
+    for n, e in geno_features():
         if n in feats:
             L.append(f"    x.{n} = {_cexpr(e)};")
     L.append("}")
@@ -646,7 +695,7 @@ def numpy_geno_stats(counts9_list, n_list=None):
             x.u3 = 1.0 / (ns * (ns - 1) * (ns - 2))
             w4 = ns * (ns - 1) * (ns - 2) * (ns - 3)
             x.w4 = np.where(ns >= 4, 1 / np.where(ns >= 4, w4, 1), 0.0)
-            for name, e in GENO_FEATURES:
+            for name, e in geno_features():
                 setattr(x, name, eval(e, {}, {"x": x}))
         fs.append(x)
     calls, stats = plan(P, geno=True)
@@ -1073,6 +1122,11 @@ def numpy_hap_stats(counts_list, n_list=None):
 def check():
     """Symbolic check of the factored forms against the reference formulas (sympy)."""
     import sympy as sp
+    for poly in _HORNER_POLYS.values():
+        e, _, g = _horner_sympy(poly)
+        loc = {f"g{i + 1}": g[i] for i in range(9)}
+        h = sp.sympify(horner_form(poly).replace("x.g", "g"), locals=loc)
+        assert sp.expand(h - e) == 0
     a = sp.symbols("a1:5")
     b = sp.symbols("b1:5")
 
