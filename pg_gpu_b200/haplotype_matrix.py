@@ -194,7 +194,7 @@ class HaplotypeMatrix:
         return windowed_r_squared(self.haplotypes, self._np(self.positions), bp_bins, percentile, rows=rows)
 
     def compute_ld_statistics_gpu_single_pop(self, bp_bins, raw=False, ac_filter=True, chunk_size="auto",
-                                             method="tc"):
+                                             method="auto"):
         """{(lo, hi): (DD, Dz, pi2)} over all haplotypes, sums if ``raw`` else means
         (haplotype_matrix.py:1592-1716).  ``chunk_size`` is accepted for compatibility: the
         parse is one library call."""
@@ -203,7 +203,7 @@ class HaplotypeMatrix:
         return self._bin_dict(bp_bins, ld_names(1), res, raw, as_tuple=True)
 
     def compute_ld_statistics_gpu_two_pops(self, bp_bins, pop1, pop2, raw=False, ac_filter=True,
-                                           chunk_size="auto", method="tc"):
+                                           chunk_size="auto", method="auto"):
         """{(lo, hi): OrderedDict of the 15 two-population statistics}
         (haplotype_matrix.py:1719-1866)."""
         m = self.apply_biallelic_filter() if ac_filter else self
@@ -211,7 +211,7 @@ class HaplotypeMatrix:
         res = m._parse(bp_bins, [sets[pop1], sets[pop2]], method)
         return self._bin_dict(bp_bins, ld_names(2), res, raw, as_tuple=False)
 
-    def compute_ld_statistics(self, bp_bins, pops=None, raw=True, ac_filter=True, method="tc"):
+    def compute_ld_statistics(self, bp_bins, pops=None, raw=True, ac_filter=True, method="auto"):
         """{(lo, hi): OrderedDict of the moments statistics} for 1..4 named populations."""
         m = self.apply_biallelic_filter() if ac_filter else self
         sets = m.sample_sets

@@ -62,11 +62,11 @@ def _compute_ld_sums(mat, pops, bins, gen_dists, max_bp_dist, use_genotypes=Fals
         data = mat.genotypes.index_select(1, keep).contiguous()
         pos = mat.positions.index_select(0, keep)
         gd = None if gen_dists is None else np.asarray(gen_dists)[keep.cpu().numpy()]
-        method = method or "tc"
+        method = method or "auto"
     else:
         mat.transfer_to_gpu()
         data, pos, gd = mat.haplotypes, mat.positions, gen_dists
-        method = method or "tc"
+        method = method or "auto"
     rows = [np.asarray(mat.sample_sets[p]) for p in pops]
     res = ld_parse(data, pos.to(torch.float64), rows, bins, genotypes=use_genotypes, method=method,
                    max_dist=float(max_bp_dist), coords=gd).numpy()
@@ -107,8 +107,9 @@ def compute_ld_statistics(vcf_file=None, rec_map_file=None, pop_file=None, pops=
                           genotype_matrix=None, accessible_bed=None, method=None):
     """moments-format LD statistics for 1-4 populations (moments_ld.py:40-203).
 
-    ``method``: "tc" (tensor-core counts, FP64 estimators; the default on both paths),
-    "tc32" (haplotypes only: FP32 estimators) or "plain" (byte-counting FP64 kernel).  ``accessible_bed`` is not supported
+    ``method``: "auto" (the default: "tc", or "plain" for shapes the tensor-core kernel
+    cannot stage), "tc" (tensor-core counts, FP64 estimators), "tc32" (haplotypes only:
+    FP32 estimators) or "plain" (byte-counting FP64 kernel).  ``accessible_bed`` is not supported
     (masking is ingest, outside this library)."""
     if pops is None:
         pops = ["pop0", "pop1"]

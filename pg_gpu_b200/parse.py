@@ -7,7 +7,10 @@ finite r^2.  Two counting/estimator methods:
 
 * ``"plain"`` -- per-pair byte counting + FP64 estimators (the reference's design);
 * ``"tc"``    -- INT8 tcgen05 Gram-product counts + FP64 estimators and bin sums;
-* ``"tc32"``  -- the same counts with FP32 estimators (FP64 bin sums).
+* ``"tc32"``  -- the same counts with FP32 estimators (FP64 bin sums);
+* ``"auto"``  -- ``"tc"``, or ``"plain"`` for the shapes the tensor-core kernel cannot stage
+  (its per-bin sums and reciprocal table must fit in shared memory beside the pipeline:
+  e.g. four genotype populations with more than 20 bins).  Both are GPU kernels.
 
 ``Pipeline`` runs a stream of same-shape parses from pinned host memory with the copies
 overlapped with the parses.
@@ -21,7 +24,8 @@ import numpy as np
 
 from . import _lib
 
-METHODS = {"plain": _lib.METHOD_PLAIN, "tc": _lib.METHOD_TC, "tc32": _lib.METHOD_TC_FP32}
+METHODS = {"plain": _lib.METHOD_PLAIN, "tc": _lib.METHOD_TC, "tc32": _lib.METHOD_TC_FP32,
+           "auto": _lib.METHOD_TC}
 
 
 def n_stats(P: int) -> int:
@@ -51,7 +55,7 @@ class Parser:
     """Reusable parse of one input shape: holds the descriptor, workspace and outputs so
     that repeated calls allocate nothing (the CUDA library itself never allocates)."""
 
-    def __init__(self, data, positions, pop_rows, edges, *, genotypes=False, method="tc", max_dist=None,
+    def __init__(self, data, positions, pop_rows, edges, *, genotypes=False, method="auto", max_dist=None,
                  coords=None, window_offsets=None, snp_block=None, n_blocks=1, device=None):
         torch = _lib.require_cuda()
         lib = _lib.load()
@@ -115,6 +119,7 @@ class Parser:
         if method not in METHODS:
             raise ValueError(f"method must be one of {sorted(METHODS)}")
         d.method = METHODS[method]
+        self.auto = method == "auto"
         self.desc = d
         ws = lib.ldk_parse_workspace_size(ctypes.byref(d))
         if ws == 0:
@@ -134,9 +139,28 @@ class Parser:
         o.r2_counts = _lib.ptr(self.out.r2_counts)
         self._o = o
 
+    def _to_plain(self, rc) -> bool:
+        """With method "auto": on the tensor-core kernel's "unsupported shape" answer,
+        switch this parse to the plain FP64 kernel (new workspace size) and say so."""
+        if not (self.auto and rc == _lib.LDK_ERR_UNSUPPORTED and self.desc.method != _lib.METHOD_PLAIN):
+            return False
+        self.desc.method = _lib.METHOD_PLAIN
+        ws = self.lib.ldk_parse_workspace_size(ctypes.byref(self.desc))
+        if ws > self.workspace.numel():
+            self.workspace = self.torch.empty(int(ws), dtype=self.torch.uint8, device=self.workspace.device)
+        return True
+
+    @property
+    def method(self) -> str:
+        """The kernel this parse runs: "tc", "tc32" or "plain"."""
+        return {_lib.METHOD_PLAIN: "plain", _lib.METHOD_TC: "tc", _lib.METHOD_TC_FP32: "tc32"}[self.desc.method]
+
     def run(self, stream=None) -> ParseResult:
-        rc = self.lib.ldk_parse(ctypes.byref(self.desc), ctypes.byref(self._o), _lib.ptr(self.workspace),
-                                self.workspace.numel(), _lib.stream_handle(stream))
+        while True:
+            rc = self.lib.ldk_parse(ctypes.byref(self.desc), ctypes.byref(self._o), _lib.ptr(self.workspace),
+                                    self.workspace.numel(), _lib.stream_handle(stream))
+            if not self._to_plain(rc):
+                break
         _lib.check(rc)
         return self.out
 
@@ -150,8 +174,12 @@ class Parser:
     # -- the split form: plan once, enqueue device work only, read the status later
     def setup(self, stream=None):
         """Write the plan (window offsets, row blocks) into the workspace; synchronises."""
-        _lib.check(self.lib.ldk_parse_setup(ctypes.byref(self.desc), _lib.ptr(self.workspace),
-                                            self.workspace.numel(), _lib.stream_handle(stream)))
+        while True:
+            rc = self.lib.ldk_parse_setup(ctypes.byref(self.desc), _lib.ptr(self.workspace),
+                                          self.workspace.numel(), _lib.stream_handle(stream))
+            if not self._to_plain(rc):
+                break
+        _lib.check(rc)
 
     def enqueue(self, stream=None) -> ParseResult:
         """Enqueue one parse (device work only; capturable).  Needs ``setup()`` first."""

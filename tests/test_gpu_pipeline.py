@@ -1,6 +1,8 @@
-"""parse.Pipeline: a stream of same-shape batches from pinned host memory, double-buffered.
-Each batch's results, copied back through the pipeline, must equal a resident Parser run on
-the same input: pair tallies bit-exact, sums to 1e-12 (FP64 sums in another order)."""
+"""Host-side parse API on the GPU.  parse.Pipeline: a stream of same-shape batches from
+pinned host memory, double-buffered; each batch's results, copied back through the pipeline,
+must equal a resident Parser run on the same input (pair tallies bit-exact, sums to 1e-12:
+FP64 sums in another order).  method="auto": the plain kernel where the tensor-core kernel
+cannot stage the shape."""
 import numpy as np
 import pytest
 
@@ -76,3 +78,29 @@ def test_pipeline_rejects_mismatched_inputs():
     with pytest.raises(ValueError):
         pipe.submit({"X": torch.from_numpy(w.data).pin_memory(),
                      "pos": torch.from_numpy(w.positions).pin_memory()}, [None])
+
+
+def test_auto_method_switches_to_plain_where_tc_cannot_stage():
+    """Four genotype populations with 30 bins exceed the tensor-core kernel's shared-memory
+    staging: "tc" refuses with LDK_ERR_UNSUPPORTED, "auto" runs the plain FP64 kernel and
+    matches it; on a shape the tensor-core kernel stages, "auto" keeps it."""
+    from pg_gpu_b200 import _lib
+    w = synth.make_config(3, scale=0.01)
+    n = w.data.shape[0]
+    q = n // 4
+    rows = [np.arange(k * q, (k + 1) * q) for k in range(4)]
+    edges = np.linspace(0, w.max_dist, 31)
+    with pytest.raises(_lib.LdkError) as e:
+        parse.Parser(w.data, w.positions, rows, edges, genotypes=True, method="tc", max_dist=w.max_dist).run()
+    assert e.value.code == _lib.LDK_ERR_UNSUPPORTED
+    auto = parse.Parser(w.data, w.positions, rows, edges, genotypes=True, method="auto", max_dist=w.max_dist)
+    got = auto.run().numpy()
+    assert auto.method == "plain"
+    want = parse.Parser(w.data, w.positions, rows, edges, genotypes=True, method="plain",
+                        max_dist=w.max_dist).run().numpy()
+    np.testing.assert_array_equal(got["pairs"], want["pairs"])
+    # the plain kernel's bin sums are atomic adds, so two runs differ in the last bits
+    np.testing.assert_allclose(got["sums"], want["sums"], rtol=1e-11, atol=1e-300)
+    kept = parse.Parser(w.data, w.positions, rows[:2], w.edges, genotypes=True, method="auto", max_dist=w.max_dist)
+    kept.run()
+    assert kept.method == "tc"
