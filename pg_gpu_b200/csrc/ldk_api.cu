@@ -60,7 +60,7 @@ int check_arch() {
 }
 
 struct Layout {
-    size_t status_off = 0, jmax_off = 0, win_off = 0, items_off = 0, hv_off = 0, total = 0;
+    size_t status_off = 0, jmax_off = 0, win_off = 0, items_off = 0, hv_off = 0, rtab_off = 0, total = 0;
     int n_items = 0;
 };
 
@@ -81,6 +81,8 @@ bool shape_of(const ldk_parse_t* d, ParseShape& sh) {
     }
     for (int p = d->n_pops; p <= LDK_MAX_POPS; ++p) sh.kofs[p] = k;
     sh.ktot = (k + 127) / 128 * 128;
+    sh.rtab_global = 0;
+    sh.rtab_global = (d->method != LDK_METHOD_PLAIN_FP64 && !sh.genotypes && tc_rtab_global(sh)) ? 1 : 0;
     return true;
 }
 
@@ -112,6 +114,10 @@ Layout layout_of(const ldk_parse_t* d, const ParseShape& sh) {
         off = align_up(off + (size_t)n_items * 2 * sizeof(int32_t), 1024);
         L.hv_off = off;
         off = align_up(off + (size_t)d->n_var * sh.planes * sh.ktot, 256);
+        if (sh.rtab_global) {
+            L.rtab_off = off;
+            off = align_up(off + (size_t)(sh.max_n + 1) * 4 * sizeof(double), 256);
+        }
     }
     L.total = off;
     return L;
@@ -197,6 +203,10 @@ int prepare(const ldk_parse_t* d, void* workspace, size_t workspace_bytes, Prepa
         set_error("bins x statistics exceed the tensor-core kernel's shared-memory staging");
         return LDK_ERR_UNSUPPORTED;
     }
+    if (d->method == LDK_METHOD_TC_FP32 && P.sh.rtab_global) {
+        set_error("population too large for the FP32-estimator method's shared-memory reciprocal table; use LDK_METHOD_TC");
+        return LDK_ERR_UNSUPPORTED;
+    }
     unsigned char* ws = static_cast<unsigned char*>(workspace);
     P.ws = ws;
     P.w.status = reinterpret_cast<unsigned*>(ws + P.L.status_off);
@@ -206,6 +216,7 @@ int prepare(const ldk_parse_t* d, void* workspace, size_t workspace_bytes, Prepa
     P.w.win_off = reinterpret_cast<int64_t*>(ws + P.L.win_off);
     P.w.items = reinterpret_cast<int32_t*>(ws + P.L.items_off);
     P.w.hv = ws + P.L.hv_off;
+    P.w.rtab = P.sh.rtab_global ? static_cast<void*>(ws + P.L.rtab_off) : nullptr;
     return LDK_OK;
 }
 
@@ -316,6 +327,7 @@ int enqueue_device(const ldk_parse_t* d, const ldk_parse_out_t* out, const Prepa
         if (prof) cudaEventRecord(g_ev[1], s);
     } else {
         if ((rc = check_cuda(launch_prep_planes(&dd, P.w, P.sh, s), "indicator planes"))) return rc;
+        if (P.w.rtab && (rc = check_cuda(launch_fill_rtab(P.w.rtab, P.sh.max_n, s), "reciprocal table"))) return rc;
         if (tune && n_variants(d, P.sh) > 1 && tuned_variant(d, P.sh) < 0) {
             if ((rc = autotune_tc(&dd, out, P, s))) return rc;
             // the candidate runs left their sums and a spent row-block counter behind

@@ -17,6 +17,8 @@ struct Scratch {
     int64_t* win_off;      // (n_windows + 1) window SNP offsets
     uint8_t* hv;           // TC path: (n_var, planes, Ktot) indicator planes
     int32_t* items;        // TC path: (n_items, 2) row blocks
+    void* rtab;            // TC haplotype path: (max_n + 1) double4 reciprocal table in the
+                           // workspace, or null when it lives in shared memory
 };
 
 struct ParseShape {
@@ -28,6 +30,8 @@ struct ParseShape {
     int ktot;                    // TC path: total K bytes (multiple of 128)
     int planes;                  // TC path: indicator planes per SNP (2 haplotype, 4 genotype)
     int max_n;                   // largest population size
+    int rtab_global;             // TC haplotype path: the reciprocal table (32 B per n_valid)
+                                 // does not fit beside the pipeline in shared memory
 };
 
 // launchers (ldk_plain.cu)
@@ -63,6 +67,8 @@ int tc_rows_per_block(const ParseShape& sh);
 int tc_planes(const ParseShape& sh);
 cudaError_t probe_peaks(double* int8_ops_per_s, double* fp64_fma_per_s, unsigned* status, cudaStream_t s);
 size_t tc_smem_bytes(const ParseShape& sh);
+bool tc_rtab_global(const ParseShape& sh);  // where the reciprocal table must live
+cudaError_t launch_fill_rtab(void* rtab, int max_n, cudaStream_t s);
 
 cudaError_t launch_build_items(const Scratch& w, int n_windows, int rows, cudaStream_t s);
 

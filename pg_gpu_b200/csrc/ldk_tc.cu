@@ -158,6 +158,27 @@ size_t tc_smem_bytes(const ParseShape& sh) {
     return sh.genotypes ? tc_smem_bytes_g<true>(sh) : tc_smem_bytes_g<false>(sh);
 }
 
+bool tc_rtab_global(const ParseShape& sh) {
+    switch (sh.P) {
+        case 1: return rtab_global_t<1>(sh);
+        case 2: return rtab_global_t<2>(sh);
+        case 3: return rtab_global_t<3>(sh);
+        default: return rtab_global_t<4>(sh);
+    }
+}
+
+namespace {
+__global__ void k_fill_rtab(double4* t, int max_n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i <= max_n) t[i] = recip_entry(i);
+}
+}  // namespace
+
+cudaError_t launch_fill_rtab(void* rtab, int max_n, cudaStream_t s) {
+    k_fill_rtab<<<(max_n + 256) / 256, 256, 0, s>>>(static_cast<double4*>(rtab), max_n);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_prep_planes(const ldk_parse_t* d, const Scratch& w, const ParseShape& sh, cudaStream_t s) {
     if (d->n_var == 0) return cudaSuccess;
     PrepArgs a;

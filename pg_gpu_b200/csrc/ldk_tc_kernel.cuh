@@ -258,6 +258,8 @@ struct TcArgs {
     unsigned long long* pairs;
     unsigned long long* r2_counts;
     unsigned* status;
+    const double4* rtab_g;  // haplotype path: reciprocal table in global memory, or null when
+                            // each CTA builds it in shared memory
 };
 
 // Shared-memory state of the persistent pipeline (one CTA).
@@ -382,7 +384,10 @@ LDK_DEV void run_mma(const Pipe& S, uint32_t tmem, const TcArgs& a, int lane) {
     __syncwarp();
 }
 
-template <int P, typename T, bool PRIV, bool GENO, int V>
+// GT: the haplotype path's reciprocal table is read from the workspace (a.rtab_g) instead of
+// being built in shared memory -- a compile-time choice, so that the shared-memory form keeps
+// its hot loop unchanged.
+template <int P, typename T, bool PRIV, bool GENO, int V, bool GT = false>
 __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
     k_parse_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcArgs a) {
     using C = Cfg<P, GENO, V>;
@@ -425,7 +430,7 @@ __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
     for (int b = threadIdx.x; b <= nb; b += blockDim.x) sedges[b] = a.edges.e[b];
     for (int idx = threadIdx.x; idx < NCOPY * SLOTS * nb * (NS + 1); idx += blockDim.x) sacc[idx] = 0.0;
     for (int idx = threadIdx.x; idx < NCOPY * SLOTS * nb * 2; idx += blockDim.x) scnt[idx] = 0u;
-    if constexpr (!GENO)
+    if constexpr (!GENO && !GT)
         for (int idx = threadIdx.x; idx <= a.max_n; idx += blockDim.x) rtab[idx] = recip_entry(idx);
     if (warp == 1) {
         tmem_alloc(&tmem_base_s, kTmemCols);
@@ -610,7 +615,8 @@ __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
 #pragma unroll
                             for (int p = 0; p < P; ++p) {
                                 hap_features<T, P>(f[p]);
-                                hap_reciprocals_from(f[p], rtab[nval[p]]);
+                                if constexpr (GT) hap_reciprocals_from(f[p], a.rtab_g[nval[p]]);
+                                else hap_reciprocals_from(f[p], rtab[nval[p]]);
                             }
                             hap_fused<T, P, 0>(f, acc);
                             T r2;
@@ -729,30 +735,50 @@ bool make_map(CUtensorMap* m, const uint8_t* planes, int64_t n_var, int ktot, in
     return r == CUDA_SUCCESS;
 }
 
+// Dynamic shared memory: pipeline stages, `ncopy` staging copies and `table` reciprocal
+// table entries (32 B each).
 template <int P, bool GENO, int V = 0>
-size_t smem_bytes_t(int nb, int max_n, int ncopy) {
+size_t smem_bytes_t(int nb, int table, int ncopy) {
     using C = Cfg<P, GENO, V>;
     return 1024 + (size_t)C::STAGES * C::STAGE_BYTES + (size_t)ncopy * C::SLOTS * nb * (C::NS + 1) * sizeof(double) +
-           (size_t)((ncopy * C::SLOTS * nb * 2 + 7) & ~7) * sizeof(unsigned) + (size_t)(max_n + 1) * sizeof(double4) + 32;
+           (size_t)((ncopy * C::SLOTS * nb * 2 + 7) & ~7) * sizeof(unsigned) + (size_t)table * sizeof(double4) + 32;
 }
+
+// Reciprocal table entries held in shared memory (none on the genotype path, none when the
+// table lives in the workspace).
+inline int smem_table(const ParseShape& sh) { return (sh.genotypes || sh.rtab_global) ? 0 : sh.max_n + 1; }
 
 // Per-warp staging copies when they fit next to the pipeline stages.
 template <int P, bool GENO, int V>
-bool private_staging(int nb, int max_n) {
-    return smem_bytes_t<P, GENO, V>(nb, max_n, Cfg<P, GENO, V>::EPI) <= kMaxSmem;
+bool private_staging(int nb, int table) {
+    return smem_bytes_t<P, GENO, V>(nb, table, Cfg<P, GENO, V>::EPI) <= kMaxSmem;
 }
 
 template <bool GENO>
 size_t tc_smem_bytes_g(const ParseShape& sh) {
+    const int t = smem_table(sh);
     switch (sh.P) {
-        case 1: return smem_bytes_t<1, GENO>(sh.n_bins, sh.max_n, 1);
-        case 2: return smem_bytes_t<2, GENO>(sh.n_bins, sh.max_n, 1);
-        case 3: return smem_bytes_t<3, GENO>(sh.n_bins, sh.max_n, 1);
-        default: return smem_bytes_t<4, GENO>(sh.n_bins, sh.max_n, 1);
+        case 1: return smem_bytes_t<1, GENO>(sh.n_bins, t, 1);
+        case 2: return smem_bytes_t<2, GENO>(sh.n_bins, t, 1);
+        case 3: return smem_bytes_t<3, GENO>(sh.n_bins, t, 1);
+        default: return smem_bytes_t<4, GENO>(sh.n_bins, t, 1);
     }
 }
 
-template <int P, typename T, bool PRIV, bool GENO, int V>
+// Haplotype path: the reciprocal table goes to the workspace when it does not fit in shared
+// memory beside the widest tile's pipeline -- with per-warp staging if that fits without
+// the table (per-warp staging matters more than a shared-memory table), else beside one
+// shared staging copy.
+template <int P>
+bool rtab_global_t(const ParseShape& sh) {
+    using C = Cfg<P, false, 0>;
+    const int nb = sh.n_bins, t = sh.max_n + 1;
+    if (smem_bytes_t<P, false, 0>(nb, t, C::EPI) <= kMaxSmem) return false;
+    if (smem_bytes_t<P, false, 0>(nb, 0, C::EPI) <= kMaxSmem) return true;
+    return smem_bytes_t<P, false, 0>(nb, t, 1) > kMaxSmem;
+}
+
+template <int P, typename T, bool PRIV, bool GENO, int V, bool GT>
 cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w,
                                      const ParseShape& sh, int n_items, cudaStream_t s) {
     using C = Cfg<P, GENO, V>;
@@ -780,19 +806,20 @@ cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t* o, co
     a.pairs = reinterpret_cast<unsigned long long*>(o->pairs);
     a.r2_counts = reinterpret_cast<unsigned long long*>(o->r2_counts);
     a.status = w.status;
+    a.rtab_g = static_cast<const double4*>(w.rtab);
     // at least half of an SM's shared memory, so that one CTA (holding all 512 TMEM
     // columns) runs per SM
-    size_t smem = smem_bytes_t<P, GENO, V>(d->n_bins, sh.max_n, PRIV ? C::EPI : 1);
+    size_t smem = smem_bytes_t<P, GENO, V>(d->n_bins, smem_table(sh), PRIV ? C::EPI : 1);
     if (smem < kMinSmem) smem = kMinSmem;
     if (smem > kMaxSmem) return cudaErrorInvalidConfiguration;
     cudaError_t e =
-        cudaFuncSetAttribute(k_parse_tc<P, T, PRIV, GENO, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_parse_tc<P, T, PRIV, GENO, V, GT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     if constexpr (C::SPLIT) {
         // the register split adds up only at kRegLaunch registers per thread; any other
         // allocation would leave setmaxnreg.inc waiting, so such a build is not launched
         cudaFuncAttributes fa;
-        e = cudaFuncGetAttributes(&fa, k_parse_tc<P, T, PRIV, GENO, V>);
+        e = cudaFuncGetAttributes(&fa, k_parse_tc<P, T, PRIV, GENO, V, GT>);
         if (e != cudaSuccess) return e;
         if (fa.numRegs != kRegLaunch) return cudaErrorInvalidKernelImage;
     }
@@ -801,10 +828,29 @@ cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t* o, co
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (n_items == 0) return cudaSuccess;
     const int grid = n_items < sms ? n_items : sms;
-    k_parse_tc<P, T, PRIV, GENO, V><<<grid, C::THREADS, smem, s>>>(mA, mB, a);
+    k_parse_tc<P, T, PRIV, GENO, V, GT><<<grid, C::THREADS, smem, s>>>(mA, mB, a);
     return cudaGetLastError();
 }
 
+
+// One population count of one tile variant: per-warp or shared staging, and the reciprocal
+// table in shared memory or (FP64 estimators, widest tile only) in the workspace.  Other
+// variants answer cudaErrorInvalidConfiguration for a workspace table, which the tile
+// autotuner reads as "does not fit this shape".
+template <int PP, bool GENO, int V, typename T>
+cudaError_t launch_staged(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w, const ParseShape& sh,
+                          int n_items, cudaStream_t s) {
+    const bool priv = private_staging<PP, GENO, V>(sh.n_bins, smem_table(sh));
+    if (!GENO && sh.rtab_global) {
+        if constexpr (!GENO && V == 0 && std::is_same<T, double>::value)
+            return priv ? launch_parse_tc_p<PP, T, true, GENO, V, true>(d, o, w, sh, n_items, s)
+                        : launch_parse_tc_p<PP, T, false, GENO, V, true>(d, o, w, sh, n_items, s);
+        else
+            return cudaErrorInvalidConfiguration;
+    }
+    return priv ? launch_parse_tc_p<PP, T, true, GENO, V, false>(d, o, w, sh, n_items, s)
+                : launch_parse_tc_p<PP, T, false, GENO, V, false>(d, o, w, sh, n_items, s);
+}
 
 // One tile variant of one path, over the population count, accumulator type and staging.
 template <bool GENO, int V, typename T>
@@ -812,9 +858,7 @@ cudaError_t dispatch_tc(const ldk_parse_t* d, const ldk_parse_out_t* o, const Sc
                         int n_items, cudaStream_t s) {
 #define LDK_TC_CASE(PP)                                                                                   \
     case PP:                                                                                              \
-        return private_staging<PP, GENO, V>(sh.n_bins, sh.max_n)                                          \
-                   ? launch_parse_tc_p<PP, T, true, GENO, V>(d, o, w, sh, n_items, s)                     \
-                   : launch_parse_tc_p<PP, T, false, GENO, V>(d, o, w, sh, n_items, s);
+        return launch_staged<PP, GENO, V, T>(d, o, w, sh, n_items, s);
     switch (sh.P) {
         LDK_TC_CASE(1)
         LDK_TC_CASE(2)
