@@ -20,7 +20,8 @@
 // Warp roles (one CTA per SM, persistent over row blocks):
 //   warp 0     TMA producer (A: row block, B: 32..128 partner SNPs, per 128-byte K chunk)
 //   warp 1     TMEM allocator and single-thread MMA issuer, double-buffered accumulators
-//   warps 4-7  epilogue, one per TMEM lane quarter: tcgen05.ld the counts, swap halves
+//   epilogue   eight warps (4..11, or 2..9; see Cfg), two per TMEM lane quarter, each
+//              taking half of every partner tile: tcgen05.ld the counts, swap halves
 //              between lane pairs, evaluate the estimators (FP64, or FP32 for
 //              LDK_METHOD_TC_FP32), sum per distance bin in registers (bins are monotone
 //              in j for a fixed i), flush each finished bin run into a per-warp FP64
