@@ -283,6 +283,34 @@ def test_parse_tc_genotypes_windows_blocks(P):
         check_parse(r, want, tol)
 
 
+@pytest.mark.parametrize("P", [1, 2, 3, 4])
+def test_parse_tc_haplotypes_windows_blocks(P):
+    """Haplotype path on tensor cores for one to four populations of unequal size (four
+    only appear here: the benchmark configurations have at most three), 64-SNP row blocks,
+    windows of 0, 1, 3 and many SNPs, bootstrap blocks, missing calls."""
+    rng = np.random.default_rng(200 + P)
+    sizes = [23, 61, 14, 40][:P]
+    n_var = 900
+    hap, _ = synth.haplotype_region(rng, sizes, n_var, n_var * 30, 0.04)
+    pos = np.cumsum(rng.integers(1, 40, size=n_var)).astype(np.float64)
+    offs = np.cumsum([0] + sizes)
+    rows = [np.arange(offs[p], offs[p + 1]) for p in range(P)]
+    wo = np.array([0, 0, 1, 4, 500, n_var])
+    # bootstrap blocks of ~150 SNPs: a 64-SNP row block of the haplotype path may span two
+    blocks = (pos // 3000).astype(np.int32)
+    nblk = int(blocks.max()) + 1
+    edges = np.array([0.0, 40.0, 150.0, 600.0, 2500.0])
+    want = O.bin_sums(hap, pos, rows, edges, max_dist=2000.0, window_offsets=wo, snp_block=blocks,
+                      n_blocks=nblk)
+    assert want["pairs"].sum() > 0
+    # plain: 1e-11 here -- 105 four-population statistics of a 14-haplotype population
+    # round a little further from the oracle's (2e-12 seen) than the 1e-12 used elsewhere
+    for method, tol in (("plain", 10 * PLAIN_RTOL), ("tc", TC_RTOL)):
+        r = parse.ld_parse(hap, pos, rows, edges, method=method, max_dist=2000.0, window_offsets=wo,
+                           snp_block=blocks, n_blocks=nblk).numpy()
+        check_parse(r, want, tol)
+
+
 def test_parse_tc_genotype_edge_cases():
     rng = np.random.default_rng(7)
     g = _genotypes(rng, 25, 300, 0.0)
