@@ -9,8 +9,9 @@ finite r^2.  Two counting/estimator methods:
 * ``"tc"``    -- INT8 tcgen05 Gram-product counts + FP64 estimators and bin sums;
 * ``"tc32"``  -- the same counts with FP32 estimators (FP64 bin sums);
 * ``"auto"``  -- ``"tc"``, or ``"plain"`` for the shapes the tensor-core kernel cannot stage
-  (its per-bin sums and reciprocal table must fit in shared memory beside the pipeline:
-  e.g. four genotype populations with more than 20 bins).  Both are GPU kernels.
+  (its per-bin sums must fit in shared memory beside the pipeline -- four genotype
+  populations with more than 20 bins do not -- and each 64-SNP (genotypes: 128-SNP) row
+  block may span at most two (four) bootstrap blocks).  Both are GPU kernels.
 
 ``Pipeline`` runs a stream of same-shape parses from pinned host memory with the copies
 overlapped with the parses.
@@ -41,6 +42,31 @@ class ParseResult:
 
     def numpy(self):
         return {k: getattr(self, k).cpu().numpy() for k in ("sums", "r2_sums", "pairs", "r2_counts")}
+
+
+# Tensor-core row blocks: SNPs per block and bootstrap blocks staged per row block
+# (csrc/ldk_tc_kernel.cuh, Cfg::ROWS and Cfg::SLOTS), haplotype and genotype paths.
+TC_ROWS = {False: 64, True: 128}
+TC_SLOTS = {False: 2, True: 4}
+
+
+def tc_blocks_fit(snp_block, window_offsets, n_var, genotypes=False) -> bool:
+    """Whether every tensor-core row block (TC_ROWS SNPs from each window start) covers at
+    most TC_SLOTS consecutive bootstrap blocks, counted from its first SNP's block -- the
+    kernel's condition (LDK_DEVERR_BLOCK_SPAN otherwise)."""
+    rows, slots = TC_ROWS[bool(genotypes)], TC_SLOTS[bool(genotypes)]
+    b = snp_block.cpu().numpy() if hasattr(snp_block, "cpu") else np.asarray(snp_block)
+    b = b.astype(np.int64).ravel()
+    wo = [0, n_var] if window_offsets is None else [int(x) for x in window_offsets]
+    for a, e in zip(wo[:-1], wo[1:]):
+        seg = b[a:e]
+        if seg.size == 0:
+            continue
+        starts = np.arange(0, seg.size, rows)
+        first = seg[starts]
+        if np.any(np.maximum.reduceat(seg, starts) - first >= slots) or np.any(np.minimum.reduceat(seg, starts) < first):
+            return False
+    return True
 
 
 def _dev(x, dtype, torch, device):
@@ -120,6 +146,8 @@ class Parser:
             raise ValueError(f"method must be one of {sorted(METHODS)}")
         d.method = METHODS[method]
         self.auto = method == "auto"
+        if self.auto and snp_block is not None and not tc_blocks_fit(snp_block, window_offsets, n_var, genotypes):
+            d.method = _lib.METHOD_PLAIN  # bootstrap blocks too small for the tensor-core staging
         self.desc = d
         ws = lib.ldk_parse_workspace_size(ctypes.byref(d))
         if ws == 0:

@@ -104,3 +104,21 @@ def test_auto_method_switches_to_plain_where_tc_cannot_stage():
     kept = parse.Parser(w.data, w.positions, rows[:2], w.edges, genotypes=True, method="auto", max_dist=w.max_dist)
     kept.run()
     assert kept.method == "tc"
+
+
+def test_auto_method_uses_plain_for_small_bootstrap_blocks():
+    """Bootstrap blocks of 20 SNPs: a 64-SNP tensor-core row block would span four, more
+    than it stages, so "tc" stops with a device error and "auto" runs the plain kernel."""
+    from pg_gpu_b200 import _lib
+    w = synth.make_config(2, scale=0.01)
+    blocks = (np.arange(w.n_var) // 20).astype(np.int32)
+    nblk = int(blocks.max()) + 1
+    kw = dict(max_dist=w.max_dist, snp_block=blocks, n_blocks=nblk)
+    with pytest.raises(_lib.LdkError):
+        parse.Parser(w.data, w.positions, w.pop_rows, w.edges, method="tc", **kw).run()
+    auto = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, method="auto", **kw)
+    got = auto.run().numpy()
+    assert auto.method == "plain"
+    want = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, method="plain", **kw).run().numpy()
+    np.testing.assert_array_equal(got["pairs"], want["pairs"])
+    np.testing.assert_allclose(got["sums"], want["sums"], rtol=1e-11, atol=1e-300)

@@ -72,3 +72,21 @@ def test_genetic_map_helpers(tmp_path):
     # slowest rate 1e-8 / bp: 1e-3 M -> 1e5 bp x 1.1
     assert abs(moments_ld._max_bp_for_r_dist(pos, gen, 1e-3) - 110_000.0) < 1e-6
     assert moments_ld._max_bp_for_r_dist(pos, gen, 10.0) == 2_000_000.0
+
+
+def test_tc_blocks_fit_matches_the_kernel_rule():
+    """Host check of the tensor-core row blocks' bootstrap-block span (64 / 128 SNPs from
+    each window start may cover at most 2 / 4 blocks from their first SNP's block)."""
+    from pg_gpu_b200.parse import tc_blocks_fit
+    n = 300
+    big = np.arange(n) // 100                      # 100-SNP blocks: a 64-SNP row block spans <= 2
+    assert tc_blocks_fit(big, None, n) and tc_blocks_fit(big, None, n, genotypes=True)
+    small = np.arange(n) // 30                     # 30-SNP blocks: 64 SNPs span 3
+    assert not tc_blocks_fit(small, None, n)
+    assert tc_blocks_fit(np.arange(n) // 40, None, n, genotypes=True)       # 128 SNPs span <= 4
+    assert not tc_blocks_fit(np.arange(n) // 30, None, n, genotypes=True)   # ... but 5 here
+    # row blocks restart at each window: windows of 60 SNPs keep 30-SNP blocks within two
+    assert tc_blocks_fit(small, [0, 60, 120, 180, 240, 300], n)
+    down = big.copy()
+    down[5] = -1                                   # a block index below the row block's first
+    assert not tc_blocks_fit(down, None, n)
