@@ -108,6 +108,17 @@ typedef struct {
     int32_t n_blocks;           /* >= 1 */
     int32_t method;             /* LDK_METHOD_* */
 } ldk_parse_t;
+/* Limits of the tensor-core methods (LDK_METHOD_TC, LDK_METHOD_TC_FP32), none of which
+ * bind LDK_METHOD_PLAIN_FP64:
+ *  - each row block -- 64 SNPs (genotypes: 128) counted from each window's first SNP --
+ *    may cover at most 2 (genotypes: 4) consecutive bootstrap blocks from its first SNP's
+ *    block; otherwise the parse stops with LDK_ERR_DEVICE and status LDK_DEVERR_BLOCK_SPAN;
+ *  - the per-bin sums of the row block's bootstrap blocks must fit in shared memory beside
+ *    the pipeline, else LDK_ERR_UNSUPPORTED (four genotype populations with more than 20
+ *    bins, three with more than 47);
+ *  - LDK_METHOD_TC_FP32 also keeps a 32-byte reciprocal entry per valid count of the
+ *    largest population in shared memory (LDK_ERR_UNSUPPORTED beyond; LDK_METHOD_TC moves
+ *    that table to the workspace instead). */
 
 typedef struct {
     double* sums;        /* (n_blocks, n_bins, n_stats) statistic sums */
