@@ -27,21 +27,26 @@ struct PrepArgs {
 
 constexpr int kPrepV = 128, kPrepK = 128;
 
-LDK_DEV uint32_t plane_bit(int8_t x, int plane, int genotypes) {
-    if (genotypes) return plane == 0 ? (x == 1) : plane == 1 ? (x == 2) : plane == 2 ? (x >= 0 && x <= 2) : 0u;
-    return plane == 0 ? (x == 1) : (x == 0 || x == 1);
-}
-
 // One block: 128 K positions (haplotypes / individuals) x 128 SNPs.  The rows of the 128 K
 // positions are resolved once; the gather reads 128-byte row segments of X (consecutive
-// threads, consecutive SNPs) into a shared tile, the scatter writes each SNP's planes as
-// 128-byte runs along K.
+// threads, consecutive SNPs) into a SNP-major shared tile, the scatter turns each 4-byte K
+// quad of a SNP into its plane bytes with byte-wise compares and writes every plane as
+// 128-byte runs along K.  Plane bytes (GENO: 4 planes, haplotypes: 2):
+//   haplotypes  h = [x == 1], v = [x in {0, 1}]
+//   genotypes   [x == 1], [x == 2], [x in {0, 1, 2}], 0
+// Padding (127) and invalid codes give 0 in every plane; invalid codes also raise
+// LDK_DEVERR_BAD_INPUT.
+template <bool GENO>
 __global__ void __launch_bounds__(256) k_prep_planes(PrepArgs a) {
-    __shared__ int8_t tile[kPrepK][kPrepV + 1];  // odd row length: the scatter's column reads hit distinct banks
+    constexpr int PL = GENO ? 4 : 2;
+    constexpr int RS = kPrepK + 4;  // bytes per SNP row: 33 words, so both the gather's byte
+                                    // stores (one SNP per lane) and the scatter's word loads
+                                    // (one K quad per lane) hit distinct banks
+    __shared__ __align__(16) int8_t tile[kPrepV * RS];
     __shared__ int srow[kPrepK];
     const int64_t v0 = (int64_t)blockIdx.x * kPrepV;
     const int k0 = blockIdx.y * kPrepK;
-    const int xmax = a.genotypes ? 2 : 1;
+    constexpr int xmax = GENO ? 2 : 1;
     for (int kk = threadIdx.x; kk < kPrepK; kk += blockDim.x) {
         const int k = k0 + kk;
         int p = 0;
@@ -51,32 +56,50 @@ __global__ void __launch_bounds__(256) k_prep_planes(PrepArgs a) {
         srow[kk] = (local >= 0 && local < np && k < a.kofs[a.P]) ? a.pop_rows[a.pop_off[p] + local] : -1;
     }
     __syncthreads();
-    // gather: tile[k][v] = X[row(k), v0 + v]; 127 marks padding
+    // gather: tile[v][k] = X[row(k), v0 + v]; 127 marks padding.  Each thread keeps one SNP
+    // column (a warp reads 32 consecutive bytes of a row) and walks every second K row, 16
+    // loads in flight.
+    constexpr int kThreads = 256, kRowStep = kThreads / kPrepV;
+    static_assert(kThreads % kPrepV == 0 && kPrepK % kRowStep == 0, "gather geometry");
     bool bad = false;
-    for (int idx = threadIdx.x; idx < kPrepK * kPrepV; idx += blockDim.x) {
-        const int kk = idx / kPrepV, vv = idx % kPrepV;
+    {
+        const int vv = threadIdx.x % kPrepV, kb = threadIdx.x / kPrepV;
         const int64_t v = v0 + vv;
-        const int row = srow[kk];
-        int8_t x = 127;
-        if (row >= 0 && v < a.n_var) {
-            x = __ldg(a.X + (int64_t)row * a.ld + v);
-            bad |= (x < -1 || x > xmax);
+        const bool vin = v < a.n_var;
+        const int8_t* col = a.X + v;
+        int8_t* trow = tile + vv * RS;
+#pragma unroll 16
+        for (int kk = kb; kk < kPrepK; kk += kRowStep) {
+            const int row = srow[kk];
+            int8_t x = 127;
+            if (row >= 0 && vin) {
+                x = __ldg(col + (int64_t)row * a.ld);
+                bad |= (x < -1 || x > xmax);
+            }
+            trow[kk] = x;
         }
-        tile[kk][vv] = x;
     }
     if (bad) atomicOr(a.status, LDK_DEVERR_BAD_INPUT);
     __syncthreads();
-    // scatter: 4 bytes of one plane per thread, coalesced along k
-    for (int idx = threadIdx.x; idx < kPrepV * a.planes * (kPrepK / 4); idx += blockDim.x) {
-        const int kq = idx % (kPrepK / 4);
-        const int plane = (idx / (kPrepK / 4)) % a.planes;
-        const int vv = idx / (a.planes * (kPrepK / 4));
+    // scatter: lane = K quad, warps stride over the SNPs
+    const int kq = threadIdx.x % 32;
+    constexpr uint32_t kOne = 0x01010101u;
+    for (int vv = threadIdx.x / 32; vv < kPrepV; vv += kThreads / 32) {
         const int64_t v = v0 + vv;
-        if (v >= a.n_var) continue;
-        uint32_t w = 0;
-#pragma unroll
-        for (int b = 0; b < 4; ++b) w |= plane_bit(tile[4 * kq + b][vv], plane, a.genotypes) << (8 * b);
-        *reinterpret_cast<uint32_t*>(a.planes_out + (v * a.planes + plane) * (int64_t)a.ktot + k0 + 4 * kq) = w;
+        if (v >= a.n_var) break;
+        const uint32_t w = *reinterpret_cast<const uint32_t*>(tile + vv * RS + 4 * kq);
+        const uint32_t eq0 = __vcmpeq4(w, 0u), eq1 = __vcmpeq4(w, kOne);
+        uint8_t* dst = a.planes_out + v * PL * (int64_t)a.ktot + k0 + 4 * kq;
+        if constexpr (GENO) {
+            const uint32_t eq2 = __vcmpeq4(w, 2u * kOne);
+            *reinterpret_cast<uint32_t*>(dst) = eq1 & kOne;
+            *reinterpret_cast<uint32_t*>(dst + a.ktot) = eq2 & kOne;
+            *reinterpret_cast<uint32_t*>(dst + 2 * (int64_t)a.ktot) = (eq0 | eq1 | eq2) & kOne;
+            *reinterpret_cast<uint32_t*>(dst + 3 * (int64_t)a.ktot) = 0u;
+        } else {
+            *reinterpret_cast<uint32_t*>(dst) = eq1 & kOne;
+            *reinterpret_cast<uint32_t*>(dst + a.ktot) = (eq0 | eq1) & kOne;
+        }
     }
 }
 
@@ -197,7 +220,8 @@ cudaError_t launch_prep_planes(const ldk_parse_t* d, const Scratch& w, const Par
     a.planes_out = w.hv;
     a.status = w.status;
     dim3 grid((unsigned)((d->n_var + kPrepV - 1) / kPrepV), (unsigned)(sh.ktot / kPrepK));
-    k_prep_planes<<<grid, 256, 0, s>>>(a);
+    if (sh.genotypes) k_prep_planes<true><<<grid, 256, 0, s>>>(a);
+    else k_prep_planes<false><<<grid, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 
