@@ -881,8 +881,19 @@ def _term_cost(A, B):
     return 1 + sum(t.count("*") + t.count(" + ") + t.count(" - ") for t in (A, B))
 
 
+# Four populations: the split the tensor-core kernel uses to divide the 105 statistics
+# between the two epilogue warps of a TMEM lane quarter, set by register pressure rather than
+# cost.  Measured (4 populations of 100-160 haplotypes, 16 bins): the cost-balanced point
+# (72) leaves one warp 72 accumulators and spills ~1.1 KB per thread, 4.1e9 pairs/s; 56
+# spills ~0.5 KB, 7.9e9 pairs/s; 60: 7.4e9.
+FUSED_SPLIT_AT = {4: 56}
+
+
 def fused_split(P):
-    """Split point K of the statistics into two contiguous halves of about equal cost."""
+    """Split point K of the statistics into two contiguous halves: of about equal cost, or
+    FUSED_SPLIT_AT[P]."""
+    if P in FUSED_SPLIT_AT:
+        return FUSED_SPLIT_AT[P]
     costs = [sum(_term_cost(A, B) for w, c, a in terms for A, B in fused_terms(c, a, w))
              for _, terms in fused_plan(P)]
     tot, run, best = sum(costs), 0, (None, 0)

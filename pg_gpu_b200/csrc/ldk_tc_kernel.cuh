@@ -472,7 +472,14 @@ __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
         unsigned* my_scnt = scnt + (PRIV ? e * SLOTS * nb * 2 : 0);
         constexpr int STEPS = GENO ? C::NJ : C::NJ / 2;   // TMEM reads per tile
         constexpr int PARTS = EPI / 4;                    // epilogue warps per lane quarter
-        constexpr int MY_STEPS = STEPS / PARTS;           // ... each reading a contiguous share
+        // SSPL (four haplotype populations): the two warps of a lane quarter split the
+        // statistics, not the partners -- both take every pair, warp part 0 accumulates
+        // statistics [0, K) and counts pairs, part 1 statistics [K, NS) and r^2 -- so that
+        // each holds about half of the 105 accumulators.
+        constexpr bool SSPL = !GENO && P == 4;
+        constexpr int K = HapFusedSplit<P>::value;
+        constexpr int NA = SSPL ? ((K > NS - K + 1 ? K : NS - K + 1)) : NS + 1;  // accumulators per lane
+        constexpr int MY_STEPS = SSPL ? STEPS : STEPS / PARTS;  // ... each reading a contiguous share
         const int part = e >> 2;
         constexpr int CREGS = (C::NJ + 31) / 32;          // partner coordinates per lane
         uint32_t tcount = 0;
@@ -508,9 +515,12 @@ __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
             // so the distance to them never decreases and each (row, bin) run is flushed
             // to shared memory once, when the lane's next partner falls past the bin's
             // upper edge (held in `nxt`).
-            T acc[NS + 1];
+            T acc[NA];
+            // statistic s of this warp's accumulators and where it goes in the staging row
+            const int na = SSPL ? (part == 0 ? K : NS - K + 1) : NS + 1;
+            const int gofs = SSPL && part == 1 ? K : 0;
 #pragma unroll
-            for (int s = 0; s <= NS; ++s) acc[s] = T(0);
+            for (int s = 0; s < NA; ++s) acc[s] = T(0);
             unsigned np = 0, nr2 = 0;
             int cur = -1;
             double nxt = sedges[0];
@@ -528,18 +538,32 @@ __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
                     double* dst = my_sacc + key * (NS + 1);
                     for (int rr = 0; rr < rounds; ++rr) {
                         if (want && rank == rr) {
+                            if constexpr (SSPL) {
 #pragma unroll
-                            for (int s = 0; s <= NS; ++s) dst[s] += (double)acc[s];
-                            my_scnt[2 * key] += np;
+                                for (int s = 0; s < NA; ++s)
+                                    if (s < na) dst[gofs + s] += (double)acc[s];
+                                if (part == 0) my_scnt[2 * key] += np;
+                            } else {
+#pragma unroll
+                                for (int s = 0; s <= NS; ++s) dst[s] += (double)acc[s];
+                                my_scnt[2 * key] += np;
+                            }
                             my_scnt[2 * key + 1] += nr2;
                         }
                         __syncwarp();
                     }
                 } else if (want) {
                     double* dst = my_sacc + key * (NS + 1);
+                    if constexpr (SSPL) {
 #pragma unroll
-                    for (int s = 0; s <= NS; ++s) atomicAdd(dst + s, (double)acc[s]);
-                    atomicAdd(my_scnt + 2 * key, np);
+                        for (int s = 0; s < NA; ++s)
+                            if (s < na) atomicAdd(dst + gofs + s, (double)acc[s]);
+                        if (part == 0) atomicAdd(my_scnt + 2 * key, np);
+                    } else {
+#pragma unroll
+                        for (int s = 0; s <= NS; ++s) atomicAdd(dst + s, (double)acc[s]);
+                        atomicAdd(my_scnt + 2 * key, np);
+                    }
                     atomicAdd(my_scnt + 2 * key + 1, nr2);
                 }
             };
@@ -561,7 +585,7 @@ __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
                 // Genotypes: one partner per step, 4 columns per region and population.
 #pragma unroll 1
                 for (int qq = 0; qq < MY_STEPS; ++qq) {
-                    const int q = part * MY_STEPS + qq;
+                    const int q = SSPL ? qq : part * MY_STEPS + qq;
                     uint32_t v[P][C::REGIONS][4];
 #pragma unroll
                     for (int p = 0; p < P; ++p)
@@ -592,7 +616,7 @@ __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
                         cur = bin_advance(sedges, nb, cur, dist);
                         nxt = cur < nb ? sedges[cur + 1] : CUDART_INF;
 #pragma unroll
-                        for (int s = 0; s <= NS; ++s) acc[s] = T(0);
+                        for (int s = 0; s < NA; ++s) acc[s] = T(0);
                         np = nr2 = 0;
                     }
                     if constexpr (!GENO) {
@@ -619,9 +643,20 @@ __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
                                 if constexpr (GT) hap_reciprocals_from(f[p], a.rtab_g[nval[p]]);
                                 else hap_reciprocals_from(f[p], rtab[nval[p]]);
                             }
-                            hap_fused<T, P, 0>(f, acc);
-                            T r2;
-                            if (hap_r2(f[0], r2)) { acc[NS] += r2; ++nr2; }
+                            if constexpr (SSPL) {
+                                if (part == 0) {
+                                    hap_fused<T, P, 1>(f, acc);
+                                } else {
+                                    hap_fused<T, P, 2>(f, acc);
+                                    T r2;
+                                    // r^2 is this part's last staged value (global index NS)
+                                    if (hap_r2(f[0], r2)) { acc[NS - K] += r2; ++nr2; }
+                                }
+                            } else {
+                                hap_fused<T, P, 0>(f, acc);
+                                T r2;
+                                if (hap_r2(f[0], r2)) { acc[NS] += r2; ++nr2; }
+                            }
                             ++np;
                         }
                     } else {
