@@ -90,3 +90,22 @@ def test_tc_blocks_fit_matches_the_kernel_rule():
     down = big.copy()
     down[5] = -1                                   # a block index below the row block's first
     assert not tc_blocks_fit(down, None, n)
+
+
+def test_genotype_horner_forms_are_exact_in_fp64():
+    """The generated Horner forms of the three single-population genotype polynomials give
+    bit-identical FP64 results to pg_gpu's expanded forms on integer cell counts (every
+    intermediate is an integer below 2^53 for counts up to 10^4)."""
+    from pg_gpu_b200.csrc import gen_estimators as G
+
+    class X:
+        pass
+
+    rng = np.random.default_rng(5)
+    x = X()
+    for m in range(1, 10):
+        setattr(x, f"g{m}", rng.integers(0, 10_000, size=20_000).astype(np.float64))
+    for poly in G._HORNER_POLYS.values():
+        want = eval(poly, {}, {"x": x})
+        got = eval(G.horner_form(poly), {}, {"x": x})
+        np.testing.assert_array_equal(got, want)
