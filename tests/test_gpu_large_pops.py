@@ -23,10 +23,14 @@ def _region(sizes, m, seed):
     return hap[:, keep].copy(), pos[keep].astype(np.float64), rows
 
 
-@pytest.mark.parametrize("sizes", [[6000], [1600, 1500, 1800]])
-def test_tc_with_reciprocal_table_in_workspace(sizes):
+@pytest.mark.parametrize("sizes,n_bins", [([6000], 16), ([1600, 1500, 1800], 16),
+                                           ([3500, 120, 90, 100], 16), ([60, 80, 70, 90], 30)])
+def test_tc_with_reciprocal_table_in_workspace(sizes, n_bins):
+    """Four populations split their statistics between the two warps of a lane quarter and,
+    with 105 statistics, flush through one shared staging copy: with a 3,500-haplotype
+    population the table goes to the workspace; the 30-bin case keeps it in shared memory."""
     hap, pos, rows = _region(sizes, 300, seed=sum(sizes))
-    edges = np.logspace(1, 5, 17)
+    edges = np.logspace(1, 5, n_bins + 1)
     kw = dict(max_dist=edges[-1])
     tc = parse.Parser(hap, pos, rows, edges, method="tc", **kw)
     got = tc.run().numpy()
