@@ -645,8 +645,9 @@ def emit_geno(P):
     feats = geno_features_needed(P)
     calls, stats = plan(P, geno=True)
     L = [f"// genotype path, P = {P}: {len(stats)} statistics from {len(calls)} distinct raw calls",
-         "template <typename T>", f"LDK_DEV void geno_features_P{P}(GenoFeat<T>& x) {{",
-         "    geno_prepare(x);"]
+         "// (PREP false: the reciprocals are already set, e.g. by geno_prepare_from)",
+         "template <typename T, bool PREP = true>", f"LDK_DEV void geno_features_P{P}(GenoFeat<T>& x) {{",
+         "    if constexpr (PREP) geno_prepare(x);"]
     for n, e in geno_features():
         if n in feats:
             L.append(f"    x.{n} = {_cexpr(e)};")
@@ -1038,12 +1039,12 @@ LDK_DEV void hap_features(HapFeat<T>& x) {
     else if constexpr (P == 3) hap_features_P3<T>(x);
     else hap_features_P4<T>(x);
 }
-template <typename T, int P>
+template <typename T, int P, bool PREP = true>
 LDK_DEV void geno_features(GenoFeat<T>& x) {
-    if constexpr (P == 1) geno_features_P1<T>(x);
-    else if constexpr (P == 2) geno_features_P2<T>(x);
-    else if constexpr (P == 3) geno_features_P3<T>(x);
-    else geno_features_P4<T>(x);
+    if constexpr (P == 1) geno_features_P1<T, PREP>(x);
+    else if constexpr (P == 2) geno_features_P2<T, PREP>(x);
+    else if constexpr (P == 3) geno_features_P3<T, PREP>(x);
+    else geno_features_P4<T, PREP>(x);
 }
 template <typename T, int P, int S = 1>
 LDK_DEV void geno_stats(const GenoFeat<T>* f, T* acc) {

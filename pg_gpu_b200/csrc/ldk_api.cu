@@ -60,7 +60,7 @@ int check_arch() {
 }
 
 struct Layout {
-    size_t status_off = 0, jmax_off = 0, win_off = 0, items_off = 0, hv_off = 0, rtab_off = 0, total = 0;
+    size_t status_off = 0, jmax_off = 0, win_off = 0, items_off = 0, hv_off = 0, rtab_off = 0, gtab_off = 0, total = 0;
     int n_items = 0;
 };
 
@@ -117,6 +117,10 @@ Layout layout_of(const ldk_parse_t* d, const ParseShape& sh) {
         if (sh.rtab_global) {
             L.rtab_off = off;
             off = align_up(off + (size_t)(sh.max_n + 1) * 4 * sizeof(double), 256);
+        }
+        if (sh.genotypes && sh.P <= 3) {  // GenoRecip per valid count
+            L.gtab_off = off;
+            off = align_up(off + (size_t)(sh.max_n + 1) * 9 * sizeof(double), 256);
         }
     }
     L.total = off;
@@ -217,6 +221,9 @@ int prepare(const ldk_parse_t* d, void* workspace, size_t workspace_bytes, Prepa
     P.w.items = reinterpret_cast<int32_t*>(ws + P.L.items_off);
     P.w.hv = ws + P.L.hv_off;
     P.w.rtab = P.sh.rtab_global ? static_cast<void*>(ws + P.L.rtab_off) : nullptr;
+    P.w.gtab = (d->method != LDK_METHOD_PLAIN_FP64 && P.sh.genotypes && P.sh.P <= 3)
+                   ? static_cast<void*>(ws + P.L.gtab_off)
+                   : nullptr;
     return LDK_OK;
 }
 
@@ -328,6 +335,7 @@ int enqueue_device(const ldk_parse_t* d, const ldk_parse_out_t* out, const Prepa
     } else {
         if ((rc = check_cuda(launch_prep_planes(&dd, P.w, P.sh, s), "indicator planes"))) return rc;
         if (P.w.rtab && (rc = check_cuda(launch_fill_rtab(P.w.rtab, P.sh.max_n, s), "reciprocal table"))) return rc;
+        if (P.w.gtab && (rc = check_cuda(launch_fill_gtab(P.w.gtab, P.sh.max_n, s), "reciprocal table"))) return rc;
         if (tune && n_variants(d, P.sh) > 1 && tuned_variant(d, P.sh) < 0) {
             if ((rc = autotune_tc(&dd, out, P, s))) return rc;
             // the candidate runs left their sums and a spent row-block counter behind

@@ -39,6 +39,32 @@ LDK_DEV void geno_prepare(GenoFeat<T>& x) {
     x.w4 = (ns >= T(4)) ? T(1) / (ns * (ns - T(1)) * (ns - T(2)) * (ns - T(3))) : T(0);
 }
 
+// geno_prepare's reciprocals as a function of n alone (n = ns on the genotype path): the
+// tensor-core parse tabulates them once per parse instead of dividing per pair.
+struct GenoRecip {
+    double inn1, invn, r1, r2, r3, u1, u2, u3, w4;
+};
+
+LDK_DEV GenoRecip geno_recip_entry(int n) {
+    GenoFeat<double> x;
+    x.n = x.ns = (double)n;
+    geno_prepare(x);
+    return GenoRecip{x.inn1, x.invn, x.r1, x.r2, x.r3, x.u1, x.u2, x.u3, x.w4};
+}
+
+// geno_prepare for n = ns, from the table entry of n (the same values bit for bit).
+LDK_DEV void geno_prepare_from(GenoFeat<double>& x, const GenoRecip* e) {
+    x.inn1 = e->inn1;
+    x.invn = e->invn;
+    x.r1 = e->r1;
+    x.r2 = e->r2;
+    x.r3 = e->r3;
+    x.u1 = e->u1;
+    x.u2 = e->u2;
+    x.u3 = e->u3;
+    x.w4 = e->w4;
+}
+
 // Pairwise-complete dosage (Rogers-Huff) r^2 from the nine cells; false where either
 // locus is constant (pg_gpu ld_statistics.py:410-443 returns NaN there).
 template <typename T>

@@ -19,6 +19,7 @@ struct Scratch {
     int32_t* items;        // TC path: (n_items, 2) row blocks
     void* rtab;            // TC haplotype path: (max_n + 1) double4 reciprocal table in the
                            // workspace, or null when it lives in shared memory
+    void* gtab;            // TC genotype path: (max_n + 1) GenoRecip reciprocal table
 };
 
 struct ParseShape {
@@ -69,6 +70,7 @@ cudaError_t probe_peaks(double* int8_ops_per_s, double* fp64_fma_per_s, unsigned
 size_t tc_smem_bytes(const ParseShape& sh);
 bool tc_rtab_global(const ParseShape& sh);  // where the reciprocal table must live
 cudaError_t launch_fill_rtab(void* rtab, int max_n, cudaStream_t s);
+cudaError_t launch_fill_gtab(void* gtab, int max_n, cudaStream_t s);
 
 cudaError_t launch_build_items(const Scratch& w, int n_windows, int rows, cudaStream_t s);
 

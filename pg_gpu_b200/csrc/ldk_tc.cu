@@ -197,6 +197,18 @@ __global__ void k_fill_rtab(double4* t, int max_n) {
 }
 }  // namespace
 
+namespace {
+__global__ void k_fill_gtab(GenoRecip* t, int max_n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i <= max_n) t[i] = geno_recip_entry(i);
+}
+}  // namespace
+
+cudaError_t launch_fill_gtab(void* gtab, int max_n, cudaStream_t s) {
+    k_fill_gtab<<<(max_n + 256) / 256, 256, 0, s>>>(static_cast<GenoRecip*>(gtab), max_n);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_fill_rtab(void* rtab, int max_n, cudaStream_t s) {
     k_fill_rtab<<<(max_n + 256) / 256, 256, 0, s>>>(static_cast<double4*>(rtab), max_n);
     return cudaGetLastError();

@@ -261,6 +261,7 @@ struct TcArgs {
     unsigned* status;
     const double4* rtab_g;  // haplotype path: reciprocal table in global memory, or null when
                             // each CTA builds it in shared memory
+    const GenoRecip* gtab;  // genotype path, P <= 3: geno_prepare's reciprocals per valid count
 };
 
 // Shared-memory state of the persistent pipeline (one CTA).
@@ -681,7 +682,14 @@ __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
                                 }
                                 geno_set_counts(f[p], cd);
                                 f[p].n = T(nv);
-                                geno_features<T, P>(f[p]);
+                                if constexpr (P <= 3) {
+                                    geno_prepare_from(f[p], a.gtab + nv);  // n = ns = nv here
+                                    geno_features<T, P, false>(f[p]);
+                                } else {
+                                    // four populations divide: the table's registers deepen
+                                    // their spill (measured 0.45 vs 0.60 Gpairs/s)
+                                    geno_features<T, P>(f[p]);
+                                }
                             }
                             geno_stats<T, P>(f, acc);
                             T r2;
@@ -843,6 +851,7 @@ cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t* o, co
     a.r2_counts = reinterpret_cast<unsigned long long*>(o->r2_counts);
     a.status = w.status;
     a.rtab_g = static_cast<const double4*>(w.rtab);
+    a.gtab = static_cast<const GenoRecip*>(w.gtab);
     // at least half of an SM's shared memory, so that one CTA (holding all 512 TMEM
     // columns) runs per SM
     size_t smem = smem_bytes_t<P, GENO, V>(d->n_bins, smem_table(sh), PRIV ? C::EPI : 1);
