@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Throughput of the B200 two-locus LD parse: SNP pairs per second.
 
-Workload (default): configuration 4 of the north-star set -- 200 windows of lognormal
+Workload (default): configuration 4, the batched windowed parse -- 200 windows of lognormal
 SNP counts (median 2,000, 200..20,000), 3 populations of 50/120/300 haplotypes, 3%
 missing, 16 log-spaced distance bins (10 bp .. 1 Mb), per-window per-bin FP64
 DD/Dz/pi2 (45 statistics), 50-kb bootstrap blocks and 100 block-bootstrap replicates.
