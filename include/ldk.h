@@ -205,13 +205,19 @@ LDK_API int ldk_ld_matrix(const int8_t* X, int64_t ld_x, int64_t n_var, const in
  * shape (population count, haplotype or genotype path, method, padded sample count) runs
  * every candidate partner-tile width twice on its own input, times the second run of each
  * with CUDA events,
- * and keeps the fastest in a process-wide table (behind a mutex); that call returns the
- * last candidate's sums (every candidate computes the same sums).  Later ldk_parse and
+ * and keeps the fastest in a process-wide table (behind a mutex); that call then clears
+ * its outputs and runs the kept width on its input.  Later ldk_parse and
  * ldk_parse_enqueue calls of the shape use the kept width; shapes never tuned use the
  * default width.  ldk_tile_width returns the width (SNPs per partner tile) a call with
  * this descriptor would use now, 0 for the plain method, or a negative status. */
 LDK_API int ldk_autotune(int enable);
 LDK_API int ldk_tile_width(const ldk_parse_t* d);
+
+/* Row blocks of the tensor-core methods (genotypes 0: haplotype path, 1: genotype path):
+ * *rows SNPs per row block, counted from each window's first SNP, and *max_blocks, the
+ * bootstrap blocks one row block may cover from its first SNP's block (more stops the
+ * parse with LDK_DEVERR_BLOCK_SPAN).  Host-only; no counterpart in pg_gpu. */
+LDK_API int ldk_tc_row_blocks(int genotypes, int32_t* rows, int32_t* max_blocks);
 
 /* Per-thread kernel timing: while enabled, ldk_parse brackets its main counting /
  * estimator kernel with CUDA events on the caller's stream; ldk_profile_last_kernel_ms

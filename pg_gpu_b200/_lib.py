@@ -80,6 +80,7 @@ EXPORTS = {
     "ldk_ld_matrix": (ctypes.c_int, [c_vp, ctypes.c_int64, ctypes.c_int64, c_vp, ctypes.c_int32, ctypes.c_int, c_vp,
                                      ctypes.c_int64, c_vp, c_vp, ctypes.c_size_t, c_vp]),
     "ldk_tile_width": (ctypes.c_int, [ctypes.POINTER(ParseDesc)]),
+    "ldk_tc_row_blocks": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]),
     "ldk_profile": (ctypes.c_int, [ctypes.c_int]),
     "ldk_profile_last_kernel_ms": (ctypes.c_double, []),
     "ldk_block_combine": (ctypes.c_int, [c_vp, ctypes.c_int64, ctypes.c_int64, c_vp, ctypes.c_int64, c_vp,
@@ -148,3 +149,11 @@ def probe_peaks(stream=None):
 def autotune(enable=True):
     """Turn tile autotuning of the tensor-core parse on or off (``ldk_autotune``)."""
     check(load().ldk_autotune(int(bool(enable))))
+
+
+def tc_row_blocks(genotypes: bool):
+    """(SNPs per tensor-core row block, bootstrap blocks one row block may cover) of the
+    haplotype or genotype path (``ldk_tc_row_blocks``; no GPU needed)."""
+    rows, blocks = ctypes.c_int32(), ctypes.c_int32()
+    check(load().ldk_tc_row_blocks(int(bool(genotypes)), ctypes.byref(rows), ctypes.byref(blocks)))
+    return rows.value, blocks.value

@@ -554,6 +554,15 @@ int ldk_tile_width(const ldk_parse_t* d) {
     return tc_tile_width(sh, v < 0 ? 0 : v);
 }
 
+int ldk_tc_row_blocks(int genotypes, int32_t* rows, int32_t* max_blocks) {
+    if (!rows || !max_blocks) { set_error("null output pointer"); return LDK_ERR_ARG; }
+    ParseShape sh{};
+    sh.genotypes = genotypes ? 1 : 0;
+    *rows = tc_rows_per_block(sh);
+    *max_blocks = tc_block_slots(sh);
+    return LDK_OK;
+}
+
 int ldk_parse_status(const void* workspace, void* stream) {
     if (!workspace) { set_error("null workspace"); return LDK_ERR_ARG; }
     return read_status(static_cast<const unsigned*>(workspace), (cudaStream_t)stream);

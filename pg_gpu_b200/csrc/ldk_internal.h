@@ -65,6 +65,7 @@ cudaError_t launch_tc_geno(const ldk_parse_t* d, const ldk_parse_out_t* o, const
                            int n_items, int variant, cudaStream_t s);
 int tc_tile_width(const ParseShape& sh, int variant);  // partners per tile of a tile variant
 int tc_rows_per_block(const ParseShape& sh);
+int tc_block_slots(const ParseShape& sh);  // bootstrap blocks one row block may cover
 int tc_planes(const ParseShape& sh);
 cudaError_t probe_peaks(double* int8_ops_per_s, double* fp64_fma_per_s, unsigned* status, cudaStream_t s);
 size_t tc_smem_bytes(const ParseShape& sh);

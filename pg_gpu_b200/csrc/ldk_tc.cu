@@ -174,6 +174,7 @@ __global__ void __launch_bounds__(512) k_probe_fp64(int iters, double b, double 
 }  // namespace
 
 int tc_rows_per_block(const ParseShape& sh) { return sh.genotypes ? Cfg<1, true>::ROWS : Cfg<1, false>::ROWS; }
+int tc_block_slots(const ParseShape& sh) { return sh.genotypes ? Cfg<1, true>::SLOTS : Cfg<1, false>::SLOTS; }
 int tc_tile_width(const ParseShape& sh, int variant) { return tile_nj(sh.P, sh.genotypes != 0, variant); }
 int tc_planes(const ParseShape& sh) { return sh.genotypes ? Cfg<1, true>::PLANES : Cfg<1, false>::PLANES; }
 

@@ -44,17 +44,12 @@ class ParseResult:
         return {k: getattr(self, k).cpu().numpy() for k in ("sums", "r2_sums", "pairs", "r2_counts")}
 
 
-# Tensor-core row blocks: SNPs per block and bootstrap blocks staged per row block
-# (csrc/ldk_tc_kernel.cuh, Cfg::ROWS and Cfg::SLOTS), haplotype and genotype paths.
-TC_ROWS = {False: 64, True: 128}
-TC_SLOTS = {False: 2, True: 4}
-
-
 def tc_blocks_fit(snp_block, window_offsets, n_var, genotypes=False) -> bool:
-    """Whether every tensor-core row block (TC_ROWS SNPs from each window start) covers at
-    most TC_SLOTS consecutive bootstrap blocks, counted from its first SNP's block -- the
-    kernel's condition (LDK_DEVERR_BLOCK_SPAN otherwise)."""
-    rows, slots = TC_ROWS[bool(genotypes)], TC_SLOTS[bool(genotypes)]
+    """Whether every tensor-core row block (``_lib.tc_row_blocks``: SNPs counted from each
+    window start) covers at most the bootstrap blocks the kernel stages per row block,
+    counted from its first SNP's block -- the kernel's condition (LDK_DEVERR_BLOCK_SPAN
+    otherwise)."""
+    rows, slots = _lib.tc_row_blocks(genotypes)
     b = snp_block.cpu().numpy() if hasattr(snp_block, "cpu") else np.asarray(snp_block)
     b = b.astype(np.int64).ravel()
     wo = [0, n_var] if window_offsets is None else [int(x) for x in window_offsets]
