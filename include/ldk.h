@@ -132,13 +132,15 @@ LDK_API size_t ldk_parse_workspace_size(const ldk_parse_t* d);
 LDK_API int ldk_parse(const ldk_parse_t* d, const ldk_parse_out_t* out, void* workspace,
               size_t workspace_bytes, void* stream);
 
-/* ldk_parse without a workspace, for callers that cannot allocate device memory (code
- * running under CUDA graph capture, or a host runtime behind a JNI / cgo / N-API layer
- * that owns no device allocator).  Scratch comes from a file-scope device array of
- * LDK_NOALLOC_SCRATCH_BYTES held by every GPU that loads the library until exit; a parse
- * needing more returns LDK_ERR_UNSUPPORTED.  The first call on a device resolves the
- * array's address: make it before any stream capture.  All calls share the array, so
- * calls that overlap on the GPU race.  No counterpart in pg_gpu. */
+/* ldk_parse without a workspace, for callers that cannot allocate device memory: a host
+ * runtime reaching this library through a JNI / cgo / N-API layer that owns no device
+ * allocator and only hands over its input and output buffers, or a host application whose
+ * memory manager forbids allocations outside its own pool.  Scratch comes from a
+ * file-scope device array of LDK_NOALLOC_SCRATCH_BYTES held by every GPU that loads the
+ * library until exit; a parse needing more returns LDK_ERR_UNSUPPORTED.  The first call
+ * on a device (and the first after that device's context was re-created) resolves the
+ * array's device address.  All calls share the array, so calls that overlap on the GPU
+ * race.  No counterpart in pg_gpu. */
 #define LDK_NOALLOC_SCRATCH_BYTES (64ull << 20)
 LDK_API int ldk_parse_noalloc(const ldk_parse_t* d, const ldk_parse_out_t* out, void* stream);
 

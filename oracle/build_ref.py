@@ -12,7 +12,9 @@ the CPU and produces golden vectors.  Nothing from the reference is copied into 
 repository: the generated C++ and the library live only under ``oracle/_ref/``
 (git-ignored).
 
-Usage: ``python oracle/build_ref.py [--reference /path/to/pg_gpu-checkout]``.
+Usage: ``python oracle/build_ref.py [--reference /path/to/pg_gpu-checkout]``.  Without
+``--reference`` the checkout is taken from the environment variable ``PG_GPU_REFERENCE``,
+else from this machine's read-only checkout below.
 """
 from __future__ import annotations
 
@@ -26,7 +28,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_OUT = os.path.join(HERE, "_ref")
-DEFAULT_REFERENCE = "/root/reference"
+DEFAULT_REFERENCE = os.environ.get("PG_GPU_REFERENCE", "/root/reference")
 
 # modules whose RawKernel strings are on the LD path
 KERNEL_MODULES = ("ld_pipeline", "haplotype_kernels", "genotype_kernels")
@@ -87,7 +89,13 @@ def collect_kernels(reference: str):
     return kernels
 
 
-def build(reference: str = DEFAULT_REFERENCE, verbose: bool = False) -> str:
+def available(reference: str | None = None) -> bool:
+    """Whether the pg_gpu checkout this recipe reads is present."""
+    return os.path.isdir(os.path.join(reference or DEFAULT_REFERENCE, "pg_gpu"))
+
+
+def build(reference: str | None = None, verbose: bool = False) -> str:
+    reference = reference or DEFAULT_REFERENCE
     if not os.path.isdir(os.path.join(reference, "pg_gpu")):
         raise FileNotFoundError(f"reference checkout not found at {reference}")
     os.makedirs(REF_OUT, exist_ok=True)

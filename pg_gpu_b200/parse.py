@@ -250,6 +250,10 @@ class Pipeline:
     so batch k + 1 is copied in while batch k is parsed and batch k - 1 copied out (three
     streams ordered by events).
 
+    Every parse clears its slot's device status word, so after each replay the word is
+    OR-ed into a per-batch device word (on the parse stream, before the slot's next
+    batch can clear it); ``status()`` checks every batch submitted since the last check.
+
     ``submit(host_inputs, host_outputs)`` enqueues one batch: ``host_outputs`` receives
     ``(sums, pairs, *after(...))`` of that batch, each a pinned host tensor of the matching
     shape; they are valid after ``drain()``.  The caller must not reuse a batch's host
@@ -272,6 +276,7 @@ class Pipeline:
         self.parsed = [torch.cuda.Event() for _ in range(slots)]
         self.free = [torch.cuda.Event() for _ in range(slots)]
         self.k = 0
+        self._batch_status = []  # (batch index, slot, device int32 copy of that batch's status word)
 
     def submit(self, host_inputs: dict, host_outputs) -> None:
         torch = self.torch
@@ -292,6 +297,8 @@ class Pipeline:
         with torch.cuda.stream(self.compute):
             self.compute.wait_event(self.ready[s])
             graph.replay()
+            # the status word sits at the start of the workspace; keep this batch's copy
+            self._batch_status.append((self.k, s, parser.workspace[:4].view(torch.int32).clone()))
             self.parsed[s].record(self.compute)
         with torch.cuda.stream(self.d2h):
             self.d2h.wait_event(self.parsed[s])
@@ -308,9 +315,19 @@ class Pipeline:
             caller.wait_stream(st)
 
     def status(self) -> None:
-        """Synchronise and raise LdkError if a slot's last parse set a device error."""
-        for parser, _, _, _ in self.slots:
-            parser.status()
+        """Synchronise and raise LdkError if any batch submitted since the last call set a
+        device error (the library decodes the word; the message names the batch)."""
+        self.torch.cuda.synchronize()
+        pending, self._batch_status = self._batch_status, []
+        for k, s, word in pending:
+            if int(word.item()) != 0:
+                parser = self.slots[s][0]
+                # hand the batch's word back to the library, which turns it into its message
+                parser.workspace[:4].view(self.torch.int32).copy_(word)
+                try:
+                    parser.status()
+                except _lib.LdkError as e:
+                    raise _lib.LdkError(e.code, f"batch {k}: {e.args[0]}") from None
 
 
 def ld_parse(data, positions, pop_rows, edges, **kw) -> ParseResult:

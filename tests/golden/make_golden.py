@@ -1,7 +1,8 @@
 """Generate the golden fixtures in this folder from the reference itself.
 
-Runs only where the pg_gpu checkout is present (default ``/root/reference``); the
-fixtures it writes are committed and are all the tests need elsewhere.
+Runs only where the pg_gpu checkout is present (``--reference``, else the checkout that
+``oracle/build_ref.py`` reads: ``PG_GPU_REFERENCE`` or its default); the fixtures it writes
+are committed and are all the tests need elsewhere.
 
 * ``im_example.npz`` -- the reference's IM example (``examples/data/im-parsing-example.vcf``
   + ``im_pop.txt``) read into the HaplotypeMatrix layout (``haplotype_matrix.py:326-329``,

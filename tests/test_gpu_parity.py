@@ -1,7 +1,7 @@
 """GPU parity: libldk (through its C ABI) against the float64 oracle and the reference's
 golden vectors.  Tolerances: counts and pair tallies bit-exact; plain FP64 path 1e-12
-relative (1e-15 absolute) per value / per bin; tensor-core path (FP32 estimators, FP64
-bin sums) 1e-6 relative per bin."""
+relative (1e-15 absolute) per value / per bin; tensor-core path (INT8 Gram counts, FP64
+estimators and bin sums) 1e-6 relative per bin."""
 import ctypes
 import os
 

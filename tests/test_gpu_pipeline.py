@@ -122,3 +122,39 @@ def test_auto_method_uses_plain_for_small_bootstrap_blocks():
     want = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, method="plain", **kw).run().numpy()
     np.testing.assert_array_equal(got["pairs"], want["pairs"])
     np.testing.assert_allclose(got["sums"], want["sums"], rtol=1e-11, atol=1e-300)
+
+
+def test_pipeline_status_reports_an_earlier_batch_error():
+    """Four batches through two slots; the second batch's bootstrap-block ids jump inside a
+    tensor-core row block (a device error, LDK_DEVERR_BLOCK_SPAN).  Its slot parses the
+    fourth, valid batch afterwards, which clears the slot's status word -- status() must
+    still raise, naming batch 1."""
+    from pg_gpu_b200 import _lib
+    w = synth.make_config(4, scale=0.004)
+    kw = dict(genotypes=w.genotypes, method="tc", max_dist=w.max_dist, window_offsets=w.window_offsets,
+              snp_block=w.snp_block, n_blocks=w.n_blocks)
+
+    def make_slot():
+        p = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, **kw)
+        return p, {"X": p.X, "pos": p.pos, "block": p.block}, None
+
+    pipe = parse.Pipeline(make_slot, slots=2)
+    x_h = torch.from_numpy(w.data.copy()).pin_memory()
+    pos_h = torch.from_numpy(w.positions.copy()).pin_memory()
+    good = torch.from_numpy(w.snp_block.copy()).pin_memory()
+    bad = torch.from_numpy((np.arange(w.n_var) % w.n_blocks).astype(np.int32)).pin_memory()
+    ref = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, **kw)
+    shapes = (tuple(ref.out.sums.shape), tuple(ref.out.pairs.shape))
+    outs = [[torch.empty(shapes[0], dtype=torch.float64).pin_memory(),
+             torch.empty(shapes[1], dtype=torch.int64).pin_memory()] for _ in range(4)]
+    for k in range(4):
+        pipe.submit({"X": x_h, "pos": pos_h, "block": bad if k == 1 else good}, outs[k])
+    pipe.drain()
+    with pytest.raises(_lib.LdkError) as e:
+        pipe.status()
+    assert e.value.code == _lib.LDK_ERR_DEVICE
+    assert "batch 1" in str(e.value) and "bootstrap blocks" in str(e.value)
+    # the error was reported once; later batches are checked afresh
+    pipe.submit({"X": x_h, "pos": pos_h, "block": good}, outs[0])
+    pipe.drain()
+    pipe.status()

@@ -1,7 +1,8 @@
-"""ldk_parse_noalloc: the parse for callers that cannot allocate device memory (code under
-CUDA graph capture, or a host runtime behind a JNI / cgo / N-API layer with no device
-allocator of its own).  Its scratch is a static device array inside the library, so
-the caller passes only inputs and outputs.
+"""ldk_parse_noalloc: the parse for callers that cannot allocate device memory (a host
+runtime behind a JNI / cgo / N-API layer with no device allocator of its own, or an
+application whose memory manager forbids allocations outside its own pool).  Its scratch
+is a static device array inside the library, so the caller passes only inputs and
+outputs.
 
 Checked through the C ABI against ldk_parse (which takes a caller workspace) on two
 calls in a row -- the array keeps the previous call's contents, so the second call
