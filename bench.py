@@ -203,7 +203,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", type=int, default=4)
     ap.add_argument("--scale", type=float, default=1.0)
-    ap.add_argument("--method", choices=["tc", "tc32", "plain"], default="tc")
+    ap.add_argument("--method", choices=["tc", "plain"], default="tc")
     ap.add_argument("--plain-steps", type=int, default=2, help="steps of the plain FP64 kernel for the ratio")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
@@ -472,7 +472,6 @@ def main():
             "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": {"tc": "u8 counts / s32 accumulate / f64 estimators",
-                      "tc32": "u8 counts / s32 accumulate / f32 estimators / f64 bin sums",
                       "plain": "i8 byte counts / f64 estimators"}[args.method],
             "data": "synthetic (seeded founder mosaics; no public dataset offline)",
             "config": {"workload": w.name, "config_index": args.config, "scale": args.scale,

@@ -41,7 +41,6 @@ extern "C" {
 /* counting / estimator method of ldk_parse */
 #define LDK_METHOD_PLAIN_FP64 0 /* per-pair byte counting + FP64 estimators (the drop-in) */
 #define LDK_METHOD_TC 1         /* INT8 tcgen05 Gram counts; exact-integer features, FP64 combination and bins */
-#define LDK_METHOD_TC_FP32 2    /* INT8 tcgen05 Gram counts; FP32 estimators, FP64 bins (error ~1e-7 of a bin's absolute mass) */
 
 LDK_API int ldk_version(void);
 LDK_API const char* ldk_last_error(void);
@@ -108,17 +107,14 @@ typedef struct {
     int32_t n_blocks;           /* >= 1 */
     int32_t method;             /* LDK_METHOD_* */
 } ldk_parse_t;
-/* Limits of the tensor-core methods (LDK_METHOD_TC, LDK_METHOD_TC_FP32), none of which
- * bind LDK_METHOD_PLAIN_FP64:
+/* Limits of the tensor-core method (LDK_METHOD_TC), none of which bind
+ * LDK_METHOD_PLAIN_FP64:
  *  - each row block -- 64 SNPs (genotypes: 128) counted from each window's first SNP --
  *    may cover at most 2 (genotypes: 4) consecutive bootstrap blocks from its first SNP's
  *    block; otherwise the parse stops with LDK_ERR_DEVICE and status LDK_DEVERR_BLOCK_SPAN;
  *  - the per-bin sums of the row block's bootstrap blocks must fit in shared memory beside
  *    the pipeline, else LDK_ERR_UNSUPPORTED (four genotype populations with more than 20
- *    bins, three with more than 47);
- *  - LDK_METHOD_TC_FP32 also keeps a 32-byte reciprocal entry per valid count of the
- *    largest population in shared memory (LDK_ERR_UNSUPPORTED beyond; LDK_METHOD_TC moves
- *    that table to the workspace instead). */
+ *    bins, three with more than 47). */
 
 typedef struct {
     double* sums;        /* (n_blocks, n_bins, n_stats) statistic sums */

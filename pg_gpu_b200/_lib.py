@@ -24,7 +24,6 @@ NOALLOC_SCRATCH_BYTES = 64 << 20
 MAX_BINS = 64
 METHOD_PLAIN = 0
 METHOD_TC = 1
-METHOD_TC_FP32 = 2
 
 c_i8p = ctypes.c_void_p
 c_vp = ctypes.c_void_p

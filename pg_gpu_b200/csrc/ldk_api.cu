@@ -60,7 +60,8 @@ int check_arch() {
 }
 
 struct Layout {
-    size_t status_off = 0, jmax_off = 0, win_off = 0, items_off = 0, hv_off = 0, rtab_off = 0, gtab_off = 0, total = 0;
+    size_t status_off = 0, jmax_off = 0, win_off = 0, items_off = 0, hv_off = 0, rtab_off = 0, gtab_off = 0,
+           fx_off = 0, fx_bytes = 0, total = 0;
     int n_items = 0;
 };
 
@@ -102,6 +103,9 @@ Layout layout_of(const ldk_parse_t* d, const ParseShape& sh) {
     off = align_up(off + (size_t)d->n_var * sizeof(int32_t), 256);
     L.win_off = off;
     off = align_up(off + (size_t)(window_count(d) + 1) * sizeof(int64_t), 256);
+    L.fx_off = off;
+    L.fx_bytes = (size_t)d->n_blocks * d->n_bins * (sh.n_stats + 1) * kFxLimbs * sizeof(unsigned long long);
+    off = align_up(off + L.fx_bytes, 256);
     if (d->method != LDK_METHOD_PLAIN_FP64) {
         int n_items = 0;
         const int rows = tc_rows_per_block(sh);
@@ -140,7 +144,7 @@ int validate(const ldk_parse_t* d) {
     for (int p = 0; p < d->n_pops; ++p)
         if (d->pop_offsets[p + 1] <= d->pop_offsets[p]) { set_error("empty population %d", p); return LDK_ERR_ARG; }
     if (d->n_blocks < 1) { set_error("n_blocks must be >= 1"); return LDK_ERR_ARG; }
-    if (d->method != LDK_METHOD_PLAIN_FP64 && d->method != LDK_METHOD_TC && d->method != LDK_METHOD_TC_FP32) {
+    if (d->method != LDK_METHOD_PLAIN_FP64 && d->method != LDK_METHOD_TC) {
         set_error("unknown method");
         return LDK_ERR_ARG;
     }
@@ -154,10 +158,6 @@ int validate(const ldk_parse_t* d) {
         for (int w = 0; w < d->n_windows; ++w)
             if (d->window_offsets[w + 1] < d->window_offsets[w]) { set_error("window_offsets must not decrease"); return LDK_ERR_ARG; }
     }
-    if (d->method == LDK_METHOD_TC_FP32 && d->genotypes) {
-        set_error("the FP32-estimator method covers the haplotype path; use LDK_METHOD_TC for genotypes");
-        return LDK_ERR_UNSUPPORTED;
-    }
     return LDK_OK;
 }
 
@@ -165,6 +165,7 @@ const char* status_text(unsigned s) {
     if (s & LDK_DEVERR_TIMEOUT) return "device wait timed out";
     if (s & LDK_DEVERR_BLOCK_RANGE) return "snp_block outside [0, n_blocks)";
     if (s & LDK_DEVERR_BLOCK_SPAN) return "a 64-SNP row block spans more than two bootstrap blocks";
+    if (s & LDK_DEVERR_ACCUM) return "a bin sum outside the fixed-point accumulator's range (|x| >= 2^63 or not finite)";
     if (s & LDK_DEVERR_BAD_INPUT) return "unsorted positions or coordinates, or allele codes outside {-1, 0, 1} (haplotypes) or {-1, 0, 1, 2} (genotypes)";
     return "device error";
 }
@@ -207,10 +208,6 @@ int prepare(const ldk_parse_t* d, void* workspace, size_t workspace_bytes, Prepa
         set_error("bins x statistics exceed the tensor-core kernel's shared-memory staging");
         return LDK_ERR_UNSUPPORTED;
     }
-    if (d->method == LDK_METHOD_TC_FP32 && P.sh.rtab_global) {
-        set_error("population too large for the FP32-estimator method's shared-memory reciprocal table; use LDK_METHOD_TC");
-        return LDK_ERR_UNSUPPORTED;
-    }
     unsigned char* ws = static_cast<unsigned char*>(workspace);
     P.ws = ws;
     P.w.status = reinterpret_cast<unsigned*>(ws + P.L.status_off);
@@ -218,6 +215,7 @@ int prepare(const ldk_parse_t* d, void* workspace, size_t workspace_bytes, Prepa
     P.w.item_counter = reinterpret_cast<int*>(ws + P.L.status_off + 128);
     P.w.jmax = reinterpret_cast<int32_t*>(ws + P.L.jmax_off);
     P.w.win_off = reinterpret_cast<int64_t*>(ws + P.L.win_off);
+    P.w.fx = reinterpret_cast<unsigned long long*>(ws + P.L.fx_off);
     P.w.items = reinterpret_cast<int32_t*>(ws + P.L.items_off);
     P.w.hv = ws + P.L.hv_off;
     P.w.rtab = P.sh.rtab_global ? static_cast<void*>(ws + P.L.rtab_off) : nullptr;
@@ -269,7 +267,7 @@ int upload_plan(const ldk_parse_t* d, const Prepared& P, cudaStream_t s, bool de
     return LDK_OK;
 }
 
-// Zeroes the outputs and the status block.
+// Zeroes the outputs, the status block and the fixed-point bin accumulators.
 int clear(const ldk_parse_t* d, const ldk_parse_out_t* out, const Prepared& P, cudaStream_t s) {
     const int nb = d->n_bins, NS = stats_of(d->n_pops);
     int rc;
@@ -277,7 +275,8 @@ int clear(const ldk_parse_t* d, const ldk_parse_out_t* out, const Prepared& P, c
         (rc = check_cuda(cudaMemsetAsync(out->r2_sums, 0, sizeof(double) * d->n_blocks * nb, s), "memset")) ||
         (rc = check_cuda(cudaMemsetAsync(out->pairs, 0, sizeof(uint64_t) * d->n_blocks * nb, s), "memset")) ||
         (rc = check_cuda(cudaMemsetAsync(out->r2_counts, 0, sizeof(uint64_t) * d->n_blocks * nb, s), "memset")) ||
-        (rc = check_cuda(cudaMemsetAsync(P.ws + P.L.status_off, 0, 256, s), "memset")))
+        (rc = check_cuda(cudaMemsetAsync(P.ws + P.L.status_off, 0, 256, s), "memset")) ||
+        (rc = check_cuda(cudaMemsetAsync(P.ws + P.L.fx_off, 0, P.L.fx_bytes, s), "memset")))
         return rc;
     return LDK_OK;
 }
@@ -312,7 +311,6 @@ int tuned_variant(const ldk_parse_t* d, const ParseShape& sh) {
 // Tile variants worth timing: the alternative only where its width differs (the FP32
 // estimators have one variant).
 int n_variants(const ldk_parse_t* d, const ParseShape& sh) {
-    if (d->method == LDK_METHOD_TC_FP32) return 1;
     return tc_tile_width(sh, 1) != tc_tile_width(sh, 0) ? 2 : 1;
 }
 
@@ -332,6 +330,7 @@ int enqueue_device(const ldk_parse_t* d, const ldk_parse_out_t* out, const Prepa
         if (prof) cudaEventRecord(g_ev[0], s);
         if ((rc = check_cuda(launch_parse_plain(&dd, out, P.w, P.sh, s), "plain parse"))) return rc;
         if (prof) cudaEventRecord(g_ev[1], s);
+        if ((rc = check_cuda(launch_fx_finish(&dd, out, P.w, P.sh.n_stats, s), "bin sums"))) return rc;
     } else {
         if ((rc = check_cuda(launch_prep_planes(&dd, P.w, P.sh, s), "indicator planes"))) return rc;
         if (P.w.rtab && (rc = check_cuda(launch_fill_rtab(P.w.rtab, P.sh.max_n, s), "reciprocal table"))) return rc;
@@ -346,6 +345,7 @@ int enqueue_device(const ldk_parse_t* d, const ldk_parse_out_t* out, const Prepa
         if ((rc = check_cuda(launch_parse_tc(&dd, out, P.w, P.sh, P.L.n_items, v < 0 ? 0 : v, s), "tensor-core parse")))
             return rc;
         if (prof) cudaEventRecord(g_ev[1], s);
+        if ((rc = check_cuda(launch_fx_finish(&dd, out, P.w, P.sh.n_stats, s), "bin sums"))) return rc;
     }
     return LDK_OK;
 }

@@ -20,6 +20,7 @@ struct Scratch {
     void* rtab;            // TC haplotype path: (max_n + 1) double4 reciprocal table in the
                            // workspace, or null when it lives in shared memory
     void* gtab;            // TC genotype path: (max_n + 1) GenoRecip reciprocal table
+    unsigned long long* fx;  // (n_blocks, n_bins, n_stats + 1, kFxLimbs) fixed-point bin sums
 };
 
 struct ParseShape {
@@ -48,6 +49,9 @@ cudaError_t launch_r_family(int which, const double* counts, const double* n_val
 cudaError_t launch_jmax(const ldk_parse_t* d, const Scratch& w, cudaStream_t s);
 cudaError_t launch_parse_plain(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w,
                                const ParseShape& sh, cudaStream_t s);
+// sums / r2_sums from the fixed-point accumulators
+cudaError_t launch_fx_finish(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w, int n_stats,
+                             cudaStream_t s);
 cudaError_t launch_block_combine(const double* block_sums, int64_t n_blocks, int64_t k,
                                  const int32_t* weights, int64_t n_rep, double* out, cudaStream_t s);
 
@@ -58,7 +62,7 @@ cudaError_t launch_parse_tc(const ldk_parse_t* d, const ldk_parse_out_t* o, cons
                             const ParseShape& sh, int n_items, int variant, cudaStream_t s);
 // the tensor-core kernel per path and tile variant (ldk_tc_hap0.cu, ldk_tc_hap1.cu, ldk_tc_geno.cu)
 cudaError_t launch_tc_hap_v0(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w, const ParseShape& sh,
-                             int n_items, bool f32, cudaStream_t s);
+                             int n_items, cudaStream_t s);
 cudaError_t launch_tc_hap_v1(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w, const ParseShape& sh,
                              int n_items, cudaStream_t s);
 cudaError_t launch_tc_geno(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w, const ParseShape& sh,

@@ -223,8 +223,7 @@ struct PlainArgs {
     const int32_t* snp_block;
     int n_blocks;
     BinEdges edges;
-    double* sums;
-    double* r2_sums;
+    unsigned long long* fx;  // fixed-point bin sums [block][bin][NS + 1][kFxLimbs] (r^2 last)
     unsigned long long* pairs;
     unsigned long long* r2_counts;
     int* row_counter;
@@ -245,10 +244,7 @@ LDK_DEV void slab_flush(const PlainArgs& a, WarpSlab<NS>& w, int blk, int lane) 
     for (int idx = lane; idx < nb * (NS + 1); idx += 32) {
         const int b = idx / (NS + 1), s = idx % (NS + 1);
         const double v = w.acc[idx];
-        if (v != 0.0) {
-            if (s < NS) atomicAdd(&a.sums[((int64_t)blk * nb + b) * NS + s], v);
-            else atomicAdd(&a.r2_sums[(int64_t)blk * nb + b], v);
-        }
+        if (v != 0.0) fx_add(a.fx + (((int64_t)blk * nb + b) * (NS + 1) + s) * kFxLimbs, v, a.status);
         w.acc[idx] = 0.0;
     }
     for (int b = lane; b < nb; b += 32) {
@@ -384,8 +380,11 @@ __global__ void __launch_bounds__(kThreads) k_parse_plain(PlainArgs a) {
                 __syncwarp();
             }
         }
+        // flush once per claimed chunk: a slab then holds the sums of one chunk's rows in a
+        // fixed order, whichever warp claimed it, so the fixed-point totals are reproducible
+        if (cur_blk >= 0) slab_flush<NS>(a, w, cur_blk, lane);
+        cur_blk = -1;
     }
-    if (cur_blk >= 0) slab_flush<NS>(a, w, cur_blk, lane);
 }
 
 template <int P, bool GENO>
@@ -420,6 +419,19 @@ __global__ void k_build_items(const int64_t* __restrict__ win_off, int n_win, in
             items[2 * k + 1] = (int32_t)r1;
             ++k;
         }
+}
+
+// sums[blk][bin][s] (s < NS) and r2_sums[blk][bin] from the fixed-point accumulators
+__global__ void k_fx_finish(const unsigned long long* __restrict__ fx, int64_t n_rows, int NS,
+                            double* __restrict__ sums, double* __restrict__ r2_sums) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_rows * (NS + 1);
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = t / (NS + 1);
+        const int s = (int)(t % (NS + 1));
+        const double v = fx_value(fx + t * kFxLimbs);
+        if (s < NS) sums[row * NS + s] = v;
+        else r2_sums[row] = v;
+    }
 }
 
 __global__ void k_block_combine(const double* __restrict__ block_sums, int64_t n_blocks, int64_t k,
@@ -505,8 +517,7 @@ cudaError_t launch_parse_plain(const ldk_parse_t* d, const ldk_parse_out_t* o, c
     a.n_blocks = d->n_blocks;
     a.edges.n_bins = d->n_bins;
     for (int b = 0; b <= LDK_MAX_BINS; ++b) a.edges.e[b] = b <= d->n_bins ? d->edges[b] : 0.0;
-    a.sums = o->sums;
-    a.r2_sums = o->r2_sums;
+    a.fx = w.fx;
     a.pairs = reinterpret_cast<unsigned long long*>(o->pairs);
     a.r2_counts = reinterpret_cast<unsigned long long*>(o->r2_counts);
     a.row_counter = w.row_counter;
@@ -527,6 +538,13 @@ cudaError_t launch_parse_plain(const ldk_parse_t* d, const ldk_parse_out_t* o, c
 
 cudaError_t launch_build_items(const Scratch& w, int n_windows, int rows, cudaStream_t s) {
     k_build_items<<<1, 1, 0, s>>>(w.win_off, n_windows, rows, w.items);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fx_finish(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w, int n_stats,
+                             cudaStream_t s) {
+    const int64_t rows = (int64_t)d->n_blocks * d->n_bins;
+    k_fx_finish<<<blocks_for(rows * (n_stats + 1)), kThreads, 0, s>>>(w.fx, rows, n_stats, o->sums, o->r2_sums);
     return cudaGetLastError();
 }
 

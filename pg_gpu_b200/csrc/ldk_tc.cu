@@ -241,8 +241,7 @@ cudaError_t launch_prep_planes(const ldk_parse_t* d, const Scratch& w, const Par
 cudaError_t launch_parse_tc(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w,
                             const ParseShape& sh, int n_items, int variant, cudaStream_t s) {
     if (sh.genotypes) return launch_tc_geno(d, o, w, sh, n_items, variant, s);
-    if (d->method == LDK_METHOD_TC_FP32) return launch_tc_hap_v0(d, o, w, sh, n_items, true, s);
-    return variant == 1 ? launch_tc_hap_v1(d, o, w, sh, n_items, s) : launch_tc_hap_v0(d, o, w, sh, n_items, false, s);
+    return variant == 1 ? launch_tc_hap_v1(d, o, w, sh, n_items, s) : launch_tc_hap_v0(d, o, w, sh, n_items, s);
 }
 
 

@@ -1,10 +1,9 @@
-// Haplotype path, default tile (FP64 and FP32 estimators).
+// Haplotype path, default tile.
 #include "ldk_tc_kernel.cuh"
 
 namespace ldk {
 cudaError_t launch_tc_hap_v0(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w, const ParseShape& sh,
-                             int n_items, bool f32, cudaStream_t s) {
-    return f32 ? dispatch_tc<false, 0, float>(d, o, w, sh, n_items, s)
-               : dispatch_tc<false, 0, double>(d, o, w, sh, n_items, s);
+                             int n_items, cudaStream_t s) {
+    return dispatch_tc<false, 0, double>(d, o, w, sh, n_items, s);
 }
 }  // namespace ldk

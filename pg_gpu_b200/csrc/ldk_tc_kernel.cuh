@@ -22,11 +22,12 @@
 //   warp 1     TMEM allocator and single-thread MMA issuer, double-buffered accumulators
 //   epilogue   eight warps (4..11, or 2..9; see Cfg), two per TMEM lane quarter, each
 //              taking half of every partner tile: tcgen05.ld the counts, swap halves
-//              between lane pairs, evaluate the estimators (FP64, or FP32 for
-//              LDK_METHOD_TC_FP32), sum per distance bin in registers (bins are monotone
+//              between lane pairs, evaluate the estimators in FP64, sum per
+//              distance bin in registers (bins are monotone
 //              in j for a fixed i), flush each finished bin run into a per-warp FP64
 //              staging copy in shared memory, and add the staged sums to the
-//              per-bootstrap-block FP64 outputs once per row block.
+//              per-bootstrap-block fixed-point accumulators once per row block (integer
+//              atomics, so the result does not depend on the order of the row blocks).
 // Every wait is bounded (LDK_DEVERR_TIMEOUT) so a fault cannot hang the GPU.
 #pragma once
 #include <cuda.h>
@@ -254,8 +255,7 @@ struct TcArgs {
     int kofs[LDK_MAX_POPS + 1];
     int max_n;             // largest population (reciprocal table size - 1)
     BinEdges edges;
-    double* sums;
-    double* r2_sums;
+    unsigned long long* fx;  // fixed-point bin sums [block][bin][NS + 1][kFxLimbs] (r^2 last)
     unsigned long long* pairs;
     unsigned long long* r2_counts;
     unsigned* status;
@@ -715,10 +715,8 @@ __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
                 const int rem = idx % (nb * (NS + 1));
                 const int bb = rem / (NS + 1), s = rem % (NS + 1);
                 const int blk = blk0 + sl;
-                if (val != 0.0 && blk < a.n_blocks) {
-                    if (s < NS) atomicAdd(&a.sums[((int64_t)blk * nb + bb) * NS + s], val);
-                    else atomicAdd(&a.r2_sums[(int64_t)blk * nb + bb], val);
-                }
+                if (val != 0.0 && blk < a.n_blocks)
+                    fx_add(a.fx + (((int64_t)blk * nb + bb) * (NS + 1) + s) * kFxLimbs, val, a.status);
             }
             for (int idx = et; idx < SLOTS * nb; idx += 32 * EPI) {
                 unsigned long long c0 = 0, c1 = 0;
@@ -845,8 +843,7 @@ cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t* o, co
     a.max_n = sh.max_n;
     a.edges.n_bins = d->n_bins;
     for (int b = 0; b <= LDK_MAX_BINS; ++b) a.edges.e[b] = b <= d->n_bins ? d->edges[b] : 0.0;
-    a.sums = o->sums;
-    a.r2_sums = o->r2_sums;
+    a.fx = w.fx;
     a.pairs = reinterpret_cast<unsigned long long*>(o->pairs);
     a.r2_counts = reinterpret_cast<unsigned long long*>(o->r2_counts);
     a.status = w.status;

@@ -108,8 +108,8 @@ def compute_ld_statistics(vcf_file=None, rec_map_file=None, pop_file=None, pops=
     """moments-format LD statistics for 1-4 populations (moments_ld.py:40-203).
 
     ``method``: "auto" (the default: "tc", or "plain" for shapes the tensor-core kernel
-    cannot stage), "tc" (tensor-core counts, FP64 estimators), "tc32" (haplotypes only:
-    FP32 estimators) or "plain" (byte-counting FP64 kernel).  ``accessible_bed`` is not supported
+    cannot stage), "tc" (tensor-core counts, FP64 estimators) or "plain" (byte-counting
+    FP64 kernel).  ``accessible_bed`` is not supported
     (masking is ingest, outside this library)."""
     if pops is None:
         pops = ["pop0", "pop1"]

@@ -7,7 +7,6 @@ finite r^2.  Two counting/estimator methods:
 
 * ``"plain"`` -- per-pair byte counting + FP64 estimators (the reference's design);
 * ``"tc"``    -- INT8 tcgen05 Gram-product counts + FP64 estimators and bin sums;
-* ``"tc32"``  -- the same counts with FP32 estimators (FP64 bin sums);
 * ``"auto"``  -- ``"tc"``, or ``"plain"`` for the shapes the tensor-core kernel cannot stage
   (its per-bin sums must fit in shared memory beside the pipeline -- four genotype
   populations with more than 20 bins do not -- and each 64-SNP (genotypes: 128-SNP) row
@@ -25,8 +24,7 @@ import numpy as np
 
 from . import _lib
 
-METHODS = {"plain": _lib.METHOD_PLAIN, "tc": _lib.METHOD_TC, "tc32": _lib.METHOD_TC_FP32,
-           "auto": _lib.METHOD_TC}
+METHODS = {"plain": _lib.METHOD_PLAIN, "tc": _lib.METHOD_TC, "auto": _lib.METHOD_TC}
 
 
 def n_stats(P: int) -> int:
@@ -175,8 +173,8 @@ class Parser:
 
     @property
     def method(self) -> str:
-        """The kernel this parse runs: "tc", "tc32" or "plain"."""
-        return {_lib.METHOD_PLAIN: "plain", _lib.METHOD_TC: "tc", _lib.METHOD_TC_FP32: "tc32"}[self.desc.method]
+        """The kernel this parse runs: "tc" or "plain"."""
+        return {_lib.METHOD_PLAIN: "plain", _lib.METHOD_TC: "tc"}[self.desc.method]
 
     def run(self, stream=None) -> ParseResult:
         while True:
