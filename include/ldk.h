@@ -106,6 +106,11 @@ typedef struct {
     const int32_t* snp_block;   /* (n_var) bootstrap block of each SNP, or NULL = all 0 */
     int32_t n_blocks;           /* >= 1 */
     int32_t method;             /* LDK_METHOD_* */
+    const int64_t* anchor_end;  /* host (n_windows) or NULL: only SNPs i < anchor_end[w] of window w
+                                   are a pair's left SNP; partners still run to the window's end.
+                                   A rank of a split parse passes its SNP slab -- its anchors and
+                                   the read-only right halo of max_dist after them -- as a window
+                                   with anchor_end at the end of its anchors. */
 } ldk_parse_t;
 /* Limits of the tensor-core method (LDK_METHOD_TC), none of which bind
  * LDK_METHOD_PLAIN_FP64:

@@ -718,7 +718,7 @@ def geno_dosage_r2(counts9):
 
 def bin_sums(data, positions, pop_rows, edges, genotypes=False, chunk=200_000,
              max_dist=None, coords=None, pair_range=None, window_offsets=None,
-             snp_block=None, n_blocks=1):
+             snp_block=None, n_blocks=1, anchor_end=None):
     """Per-bin sums of the moments-ordered statistics.
 
     Returns dict: ``sums`` (n_blocks, n_bins, n_stats), ``pairs`` (n_blocks, n_bins)
@@ -730,7 +730,8 @@ def bin_sums(data, positions, pop_rows, edges, genotypes=False, chunk=200_000,
     ``coords`` (optional, per-SNP f64) replaces positions for binning, as the
     genetic-map path does (moments_ld.py:301-311); the pair cutoff still uses
     positions and ``max_dist``.  ``pair_range`` = (lo, hi) restricts to that slice of
-    the anchor-ordered pair list (bounded CPU baselines).
+    the anchor-ordered pair list (bounded CPU baselines).  ``anchor_end`` (one per window)
+    keeps only the pairs whose left SNP lies before it (a rank's share of a split parse).
     """
     edges = np.asarray(edges, dtype=np.float64)
     nb = len(edges) - 1
@@ -741,8 +742,11 @@ def bin_sums(data, positions, pop_rows, edges, genotypes=False, chunk=200_000,
     if window_offsets is None:
         window_offsets = [0, len(positions)]
     iis, jjs = [], []
-    for a, b in zip(window_offsets[:-1], window_offsets[1:]):
+    for w, (a, b) in enumerate(zip(window_offsets[:-1], window_offsets[1:])):
         ii, jj = pairs_within_distance(positions[a:b], max_dist)
+        if anchor_end is not None:
+            keep = ii + a < anchor_end[w]
+            ii, jj = ii[keep], jj[keep]
         iis.append(ii + a)
         jjs.append(jj + a)
     ii = np.concatenate(iis) if iis else np.empty(0, np.int64)

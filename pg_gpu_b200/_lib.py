@@ -46,6 +46,7 @@ class ParseDesc(ctypes.Structure):
         ("max_dist", ctypes.c_double), ("n_bins", ctypes.c_int32),
         ("edges", ctypes.c_double * (MAX_BINS + 1)), ("window_offsets", c_vp), ("n_windows", ctypes.c_int32),
         ("snp_block", c_vp), ("n_blocks", ctypes.c_int32), ("method", ctypes.c_int32),
+        ("anchor_end", c_vp),
     ]
 
 

@@ -94,6 +94,11 @@ int64_t window_bound(const ldk_parse_t* d, int w) {
     return w == 0 ? 0 : d->n_var;
 }
 
+// End of window w's anchors (left SNPs of its pairs).
+int64_t anchor_bound(const ldk_parse_t* d, int w) {
+    return d->anchor_end ? d->anchor_end[w] : window_bound(d, w + 1);
+}
+
 Layout layout_of(const ldk_parse_t* d, const ParseShape& sh) {
     Layout L;
     size_t off = 0;
@@ -101,8 +106,8 @@ Layout layout_of(const ldk_parse_t* d, const ParseShape& sh) {
     off += 256;
     L.jmax_off = off;
     off = align_up(off + (size_t)d->n_var * sizeof(int32_t), 256);
-    L.win_off = off;
-    off = align_up(off + (size_t)(window_count(d) + 1) * sizeof(int64_t), 256);
+    L.win_off = off;  // window offsets, then anchor ends
+    off = align_up(off + (size_t)(2 * window_count(d) + 1) * sizeof(int64_t), 256);
     L.fx_off = off;
     L.fx_bytes = (size_t)d->n_blocks * d->n_bins * (sh.n_stats + 1) * kFxLimbs * sizeof(unsigned long long);
     off = align_up(off + L.fx_bytes, 256);
@@ -110,7 +115,7 @@ Layout layout_of(const ldk_parse_t* d, const ParseShape& sh) {
         int n_items = 0;
         const int rows = tc_rows_per_block(sh);
         for (int w = 0; w < window_count(d); ++w) {
-            const int64_t m = window_bound(d, w + 1) - window_bound(d, w);
+            const int64_t m = anchor_bound(d, w) - window_bound(d, w);
             n_items += (int)((m + rows - 1) / rows);
         }
         L.n_items = n_items;
@@ -158,6 +163,12 @@ int validate(const ldk_parse_t* d) {
         for (int w = 0; w < d->n_windows; ++w)
             if (d->window_offsets[w + 1] < d->window_offsets[w]) { set_error("window_offsets must not decrease"); return LDK_ERR_ARG; }
     }
+    if (d->anchor_end)
+        for (int w = 0; w < window_count(d); ++w)
+            if (d->anchor_end[w] < window_bound(d, w) || d->anchor_end[w] > window_bound(d, w + 1)) {
+                set_error("anchor_end[%d] outside its window", w);
+                return LDK_ERR_ARG;
+            }
     return LDK_OK;
 }
 
@@ -215,6 +226,7 @@ int prepare(const ldk_parse_t* d, void* workspace, size_t workspace_bytes, Prepa
     P.w.item_counter = reinterpret_cast<int*>(ws + P.L.status_off + 128);
     P.w.jmax = reinterpret_cast<int32_t*>(ws + P.L.jmax_off);
     P.w.win_off = reinterpret_cast<int64_t*>(ws + P.L.win_off);
+    P.w.anc_end = P.w.win_off + window_count(d) + 1;
     P.w.fx = reinterpret_cast<unsigned long long*>(ws + P.L.fx_off);
     P.w.items = reinterpret_cast<int32_t*>(ws + P.L.items_off);
     P.w.hv = ws + P.L.hv_off;
@@ -239,8 +251,10 @@ int check_outputs(const ldk_parse_out_t* out) {
 // the device in window order.
 int upload_plan(const ldk_parse_t* d, const Prepared& P, cudaStream_t s, bool device_items) {
     int rc;
-    std::vector<int64_t> woff(window_count(d) + 1);
-    for (int k = 0; k <= window_count(d); ++k) woff[k] = window_bound(d, k);
+    const int nw = window_count(d);
+    std::vector<int64_t> woff(2 * nw + 1);  // window offsets, then anchor ends (the workspace layout)
+    for (int k = 0; k <= nw; ++k) woff[k] = window_bound(d, k);
+    for (int k = 0; k < nw; ++k) woff[nw + 1 + k] = anchor_bound(d, k);
     if ((rc = check_cuda(cudaMemcpyAsync(P.w.win_off, woff.data(), woff.size() * sizeof(int64_t),
                                          cudaMemcpyHostToDevice, s), "upload windows")))
         return rc;
@@ -255,11 +269,13 @@ int upload_plan(const ldk_parse_t* d, const Prepared& P, cudaStream_t s, bool de
     });
     std::vector<int32_t> items;
     items.reserve((size_t)P.L.n_items * 2);
-    for (int wi : order)
-        for (int64_t r0 = woff[wi]; r0 < woff[wi + 1]; r0 += rows) {
+    for (int wi : order) {
+        const int64_t ae = anchor_bound(d, wi);
+        for (int64_t r0 = woff[wi]; r0 < ae; r0 += rows) {
             items.push_back((int32_t)r0);
-            items.push_back((int32_t)std::min<int64_t>(r0 + rows, woff[wi + 1]));
+            items.push_back((int32_t)std::min<int64_t>(r0 + rows, ae));
         }
+    }
     if (!items.empty() &&
         (rc = check_cuda(cudaMemcpyAsync(P.w.items, items.data(), items.size() * sizeof(int32_t),
                                          cudaMemcpyHostToDevice, s), "upload row blocks")))

@@ -15,6 +15,7 @@ struct Scratch {
     int* item_counter;     // dynamic row-block counter of the tensor-core parse
     int32_t* jmax;         // (n_var) exclusive end of each SNP's partner range
     int64_t* win_off;      // (n_windows + 1) window SNP offsets
+    int64_t* anc_end;      // (n_windows) end of each window's anchor SNPs
     uint8_t* hv;           // TC path: (n_var, planes, Ktot) indicator planes
     int32_t* items;        // TC path: (n_items, 2) row blocks
     void* rtab;            // TC haplotype path: (max_n + 1) double4 reciprocal table in the

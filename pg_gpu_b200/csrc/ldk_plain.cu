@@ -178,11 +178,12 @@ __global__ void k_r_family(int which, const double* __restrict__ counts, const d
 }
 
 // ---------------------------------------------------------------------------
-// pair ranges: jmax[i] = end of SNP i's partners (cutoff on pos, window end)
+// pair ranges: jmax[i] = end of SNP i's partners (cutoff on pos, window end); i + 1 for
+// SNPs after their window's anchor end (a split parse's right halo)
 // ---------------------------------------------------------------------------
 
 __global__ void k_jmax(const double* __restrict__ pos, const double* __restrict__ coord, int64_t n_var, const int64_t* __restrict__ win_off,
-                       int n_win, double max_dist, const int32_t* __restrict__ snp_block, int n_blocks,
+                       const int64_t* __restrict__ anc_end, int n_win, double max_dist, const int32_t* __restrict__ snp_block, int n_blocks,
                        int32_t* __restrict__ jmax, unsigned* __restrict__ status) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_var;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -198,7 +199,7 @@ __global__ void k_jmax(const double* __restrict__ pos, const double* __restrict_
             const int64_t m = (a + b) >> 1;
             if (pos[m] <= lim) a = m + 1; else b = m;
         }
-        jmax[i] = (int32_t)a;
+        jmax[i] = (int32_t)(i < anc_end[lo] ? a : i + 1);  // SNPs past the anchors have no pairs of their own
         if (i + 1 < we && pos[i + 1] < pos[i]) atomicOr(status, LDK_DEVERR_BAD_INPUT);
         if (coord && i + 1 < we && coord[i + 1] < coord[i]) atomicOr(status, LDK_DEVERR_BAD_INPUT);
         if (snp_block) {
@@ -408,14 +409,16 @@ cudaError_t launch_parse_plain_t(const PlainArgs& a, int nb, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-// Row blocks of 64 SNPs per window, in window order (one thread: a setup step).
-__global__ void k_build_items(const int64_t* __restrict__ win_off, int n_win, int rows, int32_t* __restrict__ items) {
+// Row blocks of 64 (genotypes: 128) anchor SNPs per window, in window order (one thread: a
+// setup step).
+__global__ void k_build_items(const int64_t* __restrict__ win_off, const int64_t* __restrict__ anc_end, int n_win,
+                              int rows, int32_t* __restrict__ items) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     int k = 0;
     for (int wi = 0; wi < n_win; ++wi)
-        for (int64_t r0 = win_off[wi]; r0 < win_off[wi + 1]; r0 += rows) {
+        for (int64_t r0 = win_off[wi]; r0 < anc_end[wi]; r0 += rows) {
             items[2 * k] = (int32_t)r0;
-            const int64_t r1 = r0 + rows < win_off[wi + 1] ? r0 + rows : win_off[wi + 1];
+            const int64_t r1 = r0 + rows < anc_end[wi] ? r0 + rows : anc_end[wi];
             items[2 * k + 1] = (int32_t)r1;
             ++k;
         }
@@ -498,7 +501,8 @@ cudaError_t launch_r_family(int which, const double* counts, const double* n_val
 
 cudaError_t launch_jmax(const ldk_parse_t* d, const Scratch& w, cudaStream_t s) {
     if (d->n_var == 0) return cudaSuccess;
-    k_jmax<<<blocks_for(d->n_var), kThreads, 0, s>>>(d->pos, d->coord, d->n_var, w.win_off, d->n_windows, d->max_dist,
+    k_jmax<<<blocks_for(d->n_var), kThreads, 0, s>>>(d->pos, d->coord, d->n_var, w.win_off, w.anc_end, d->n_windows,
+                                                      d->max_dist,
                                                       d->snp_block, d->n_blocks, w.jmax, w.status);
     return cudaGetLastError();
 }
@@ -537,7 +541,7 @@ cudaError_t launch_parse_plain(const ldk_parse_t* d, const ldk_parse_out_t* o, c
 }
 
 cudaError_t launch_build_items(const Scratch& w, int n_windows, int rows, cudaStream_t s) {
-    k_build_items<<<1, 1, 0, s>>>(w.win_off, n_windows, rows, w.items);
+    k_build_items<<<1, 1, 0, s>>>(w.win_off, w.anc_end, n_windows, rows, w.items);
     return cudaGetLastError();
 }
 

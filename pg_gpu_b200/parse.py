@@ -75,7 +75,7 @@ class Parser:
     that repeated calls allocate nothing (the CUDA library itself never allocates)."""
 
     def __init__(self, data, positions, pop_rows, edges, *, genotypes=False, method="auto", max_dist=None,
-                 coords=None, window_offsets=None, snp_block=None, n_blocks=1, device=None):
+                 coords=None, window_offsets=None, snp_block=None, n_blocks=1, anchor_end=None, device=None):
         torch = _lib.require_cuda()
         lib = _lib.load()
         device = torch.device(device or "cuda")
@@ -133,6 +133,14 @@ class Parser:
         else:
             d.window_offsets = None
             d.n_windows = 1
+        if anchor_end is not None:
+            ae = np.asarray(anchor_end, dtype=np.int64).ravel()
+            if ae.size != d.n_windows:
+                raise ValueError("anchor_end needs one entry per window")
+            self._anc = (ctypes.c_int64 * len(ae))(*ae.tolist())
+            d.anchor_end = ctypes.cast(self._anc, ctypes.c_void_p)
+        else:
+            d.anchor_end = None
         d.snp_block = _lib.ptr(self.block)
         d.n_blocks = self.n_blocks
         if method not in METHODS:

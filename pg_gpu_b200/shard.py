@@ -1,11 +1,19 @@
-"""Splitting a batched parse across ranks (one process per GPU).
+"""Splitting a parse across ranks (one process per GPU).
 
-Pairs never cross windows, so whole windows are the unit: ``shard_windows`` assigns
-them to ranks by greedy pair-count balance (largest first), and ``combine_bins`` sums
-the ranks' per-bin (or per-block) float64 outputs with one all-reduce -- the only
-exchange the path has, a few KB to MB.  Bootstrap blocks keep their global ids, so
-per-block sums from different ranks land in disjoint rows and the all-reduce
-concatenates them.
+Two units, both with no exchange during the parse:
+
+* whole windows (many windows, e.g. a batch of genome windows): ``shard_windows``
+  assigns them to ranks by greedy pair-count balance (largest first);
+* anchor ranges (one long window, e.g. a chromosome): ``split_anchors`` cuts the
+  sequence of left SNPs into contiguous ranges of about equal pair count; a rank holds its
+  anchors plus a read-only right halo -- the SNPs up to ``max_dist`` after its last anchor,
+  which its pairs reach -- and parses that slab with ``anchor_end`` marking where its
+  anchors stop (``ldk_parse_t.anchor_end``).  This is the unit of pg_gpu's own pair chunks
+  (anchor blocks, ``ld_pipeline.py:57-122``), made contiguous so each rank reads one slab.
+
+``combine_bins`` sums the ranks' per-bin (or per-block) float64 outputs with one
+all-reduce -- the only exchange the path has, a few KB to MB.  Bootstrap blocks keep their
+global ids, so per-block sums from different ranks land in the right rows.
 """
 from __future__ import annotations
 
@@ -52,3 +60,59 @@ def combine_bins(local, group=None):
     if dist.is_available() and dist.is_initialized() and dist.get_world_size(group) > 1:
         dist.all_reduce(local, op=dist.ReduceOp.SUM, group=group)
     return local
+
+
+def partner_ends(positions, window_offsets, max_dist):
+    """jmax[i]: one past the last partner of SNP i (pos[j] - pos[i] <= max_dist, same window),
+    the pair generator's range (ld_pipeline.py:57-122)."""
+    pos = np.asarray(positions, dtype=np.float64)
+    jmax = np.empty(len(pos), dtype=np.int64)
+    for a, b in zip(window_offsets[:-1], window_offsets[1:]):
+        jmax[a:b] = a + np.searchsorted(pos[a:b], pos[a:b] + max_dist, side="right")
+    return jmax
+
+
+def split_anchors(positions, window_offsets, max_dist, world_size, align=64):
+    """Per rank, its segments ``(window, anchor_start, anchor_end, halo_end)`` in global SNP
+    indices: contiguous anchor ranges of about equal pair count over the windows in order,
+    cut at multiples of ``align`` SNPs from a window's start (the tensor-core kernel's row
+    block, so a split does not change which SNPs share a row block).  A rank's pairs are
+    those with their left SNP in ``[anchor_start, anchor_end)``; its partners end before
+    ``halo_end``."""
+    window_offsets = [int(x) for x in window_offsets]
+    n = window_offsets[-1]
+    jmax = partner_ends(positions, window_offsets, max_dist)
+    per_snp = np.maximum(0, jmax - np.arange(n) - 1)
+    cum = np.concatenate([[0], np.cumsum(per_snp)])
+    total = int(cum[-1])
+    starts = np.asarray(window_offsets[:-1], dtype=np.int64)
+    cuts = [0]
+    for r in range(1, world_size):
+        c = int(np.searchsorted(cum, total * r / world_size, side="left"))
+        w = max(0, int(np.searchsorted(starts, c, side="right")) - 1)  # window holding SNP c
+        w0, w1 = window_offsets[w], window_offsets[w + 1]
+        c = min(w1, w0 + int(round((c - w0) / align)) * align)
+        cuts.append(max(cuts[-1], c))
+    cuts.append(n)
+    plans = []
+    for r in range(world_size):
+        lo, hi = cuts[r], cuts[r + 1]
+        seg = []
+        for w, (w0, w1) in enumerate(zip(window_offsets[:-1], window_offsets[1:])):
+            a, e = max(lo, w0), min(hi, w1)
+            if a < e:
+                seg.append((w, a, e, max(e, int(jmax[e - 1]))))
+        plans.append(seg)
+    return plans
+
+
+def slab_of(segments):
+    """A rank's input slab: global SNP indices, local window offsets and local anchor ends
+    (the ``window_offsets`` / ``anchor_end`` of its parse)."""
+    idx, offs, ends = [], [0], []
+    for _, a, e, h in segments:
+        idx.append(np.arange(a, h))
+        ends.append(offs[-1] + (e - a))
+        offs.append(offs[-1] + (h - a))
+    snps = np.concatenate(idx) if idx else np.zeros(0, np.int64)
+    return snps, np.asarray(offs, dtype=np.int64), np.asarray(ends, dtype=np.int64)
