@@ -2,8 +2,10 @@
 max_dist) parsed on its own through the library with ``anchor_end``, and the outputs summed
 -- what the ranks of a multi-GPU run do, here one after another on one GPU (the rank parses
 never wait on one another).  Against one parse of the whole input: pair tallies
-bit-exact, sums to 1e-12 (the final sum of the rank outputs adds FP64 totals in another
-grouping)."""
+bit-exact, sums to 1e-12 on the tensor-core path (a rank's row blocks are the whole
+parse's; only the final sum of the rank outputs adds FP64 totals in another grouping) and
+1e-11 on the plain path (a rank's 8-SNP row chunks start after the halos of its earlier
+window segments, so its FP64 partial sums group pairs differently; cancelling bins)."""
 import numpy as np
 import pytest
 
@@ -44,7 +46,7 @@ def test_anchor_split_matches_whole_parse(cfg, scale, method, world):
         np.testing.assert_array_equal(got[k], want[k])
     assert want["pairs"].sum() > 0
     for k in ("sums", "r2_sums"):
-        np.testing.assert_allclose(got[k], want[k], rtol=1e-12, atol=1e-300)
+        np.testing.assert_allclose(got[k], want[k], rtol=1e-12 if method == "tc" else 1e-11, atol=1e-300)
 
 
 def test_anchor_end_validation():
