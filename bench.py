@@ -116,24 +116,38 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 
 def _cpu_task(args):
-    data, pos, pop_rows, edges, max_dist, n_pairs, genotypes = args
+    data, pos, pop_rows, edges, max_dist, n_anchor, genotypes = args
     os.environ.setdefault("OMP_NUM_THREADS", "1")
     from oracle import ld_oracle as O
     t0 = time.perf_counter()
-    r = O.bin_sums(data, pos, pop_rows, edges, genotypes=genotypes, max_dist=max_dist, pair_range=(0, n_pairs))
-    return min(n_pairs, r["n_pairs"]), time.perf_counter() - t0
+    r = O.bin_sums(data, pos, pop_rows, edges, genotypes=genotypes, max_dist=max_dist, anchor_end=[n_anchor])
+    return r["n_pairs"], time.perf_counter() - t0
 
 
-def cpu_sample_tasks(w, workers, pairs_per_worker):
-    """One task per worker: the first pairs of a window of <= 3,000 SNPs."""
-    offs = w.window_offsets if w.window_offsets is not None else np.array([0, w.n_var])
-    cand = [k for k in range(len(offs) - 1) if 200 <= offs[k + 1] - offs[k] <= 3000] or [0]
+def cpu_sample_tasks(w, workers, pairs_per_worker, seed=0):
+    """One task per worker: all pairs of a run of consecutive anchor SNPs (every partner,
+    so the whole distance range) starting at a SNP drawn in proportion to its pair count,
+    i.e. pairs are sampled where the workload has them, over full-size windows.  A task is
+    the anchors' slab: the anchors plus the partners after them."""
+    from pg_gpu_b200 import shard
+    offs = [0, w.n_var] if w.window_offsets is None else [int(x) for x in w.window_offsets]
+    jmax = shard.partner_ends(w.positions, offs, w.max_dist)
+    per = np.maximum(0, jmax - np.arange(w.n_var) - 1).astype(np.float64)
+    win = np.zeros(w.n_var, np.int64)
+    for k, (a, b) in enumerate(zip(offs[:-1], offs[1:])):
+        win[a:b] = k
+    rng = np.random.default_rng(seed)
     tasks = []
-    for t in range(workers):
-        k = cand[t % len(cand)]
-        a, b = int(offs[k]), int(offs[k + 1])
-        tasks.append((np.ascontiguousarray(w.data[:, a:b]), w.positions[a:b].copy(), w.pop_rows, w.edges,
-                      w.max_dist, pairs_per_worker, bool(w.genotypes)))
+    for _ in range(workers):
+        a = int(rng.choice(w.n_var, p=per / per.sum()))
+        end = offs[win[a] + 1]
+        e, got = a, 0
+        while e < end and got < pairs_per_worker:
+            got += int(per[e])
+            e += 1
+        h = max(e, int(jmax[e - 1]))
+        tasks.append((np.ascontiguousarray(w.data[:, a:h]), w.positions[a:h].copy(), w.pop_rows, w.edges,
+                      w.max_dist, e - a, bool(w.genotypes)))
     return tasks
 
 
@@ -156,14 +170,15 @@ def _noop(_):
     return 0
 
 
-def run_cpu_sample(w, seconds, workers=None, pool=None):
-    """Time the oracle on ~``seconds`` of CPU work per worker; pairs/s over all workers."""
+def run_cpu_sample(w, seconds, workers=None, pool=None, seed=0):
+    """Time the oracle on ~``seconds`` of CPU work per worker; pairs/s over all workers (a
+    rate measured on a sample: the full workload's CPU time is extrapolated from it)."""
     workers = workers or cpu_cores()
-    probe = cpu_sample_tasks(w, 1, 20_000)[0]
+    probe = cpu_sample_tasks(w, 1, 20_000, seed=10_000 + seed)[0]
     n, dt = _cpu_task(probe)
     rate = n / max(dt, 1e-9)
     per_worker = max(20_000, int(rate * seconds))
-    tasks = cpu_sample_tasks(w, workers, per_worker)
+    tasks = cpu_sample_tasks(w, workers, per_worker, seed=seed)
     own = pool is None
     if own:
         pool = cpu_pool(workers)
@@ -504,9 +519,12 @@ def main():
             line["parity"] = parity
         if cpu:
             line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["workers"], "kind": "port",
-                                    "sample": f"oracle (NumPy restatement of pg_gpu's path) on the first "
-                                              f"{cpu['per_worker_pairs']} pairs of one window per worker, "
-                                              f"{cpu['workers']} spawn workers, {cpu['wall_s']:.1f} s wall"}
+                                    "extrapolated": True,
+                                    "sample": f"oracle (NumPy restatement of pg_gpu's path): per worker all pairs "
+                                              f"of ~{cpu['per_worker_pairs']} consecutive-anchor pairs (every "
+                                              f"distance) at a pair-weighted random SNP of the full workload, "
+                                              f"{cpu['workers']} spawn workers, {cpu['wall_s']:.1f} s wall; the "
+                                              f"rate extrapolates the full workload's CPU time"}
         print(json.dumps(line), flush=True)
     if ws > 1:
         dist.destroy_process_group()
@@ -589,13 +607,14 @@ def run_reference(args, ws, rank):
         return
     w = make_workload(args.config, args.scale, 0)
     cores = cpu_cores()
-    per_step = max(5.0, min(args.cpu_seconds, 20.0))
+    # each step a bounded sample (~4 s of every core), so that K + W steps end in a few minutes
+    per_step = max(2.0, min(args.cpu_seconds, 200.0 / max(1, args.steps + args.warmup)) / 4.0)
     pool = cpu_pool(cores)
-    for _ in range(max(0, min(args.warmup, 1))):
-        run_cpu_sample(w, 2.0, cores, pool)
+    for k in range(max(0, min(args.warmup, 1))):
+        run_cpu_sample(w, 1.0, cores, pool, seed=100 + k)
     vals, pairs, wall = [], 0, 0.0
-    for _ in range(args.steps):
-        r = run_cpu_sample(w, per_step, cores, pool)
+    for k in range(args.steps):
+        r = run_cpu_sample(w, per_step, cores, pool, seed=k)
         vals.append(r["value"])
         pairs += r["pairs"]
         wall += r["wall_s"]
@@ -606,8 +625,10 @@ def run_reference(args, ws, rank):
             "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded founder mosaics)",
             "config": {"workload": w.name, "config_index": args.config, "scale": args.scale},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"oracle on the first pairs of one window per worker, {cores} workers, "
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "extrapolated": True,
+                             "sample": f"oracle (NumPy restatement of pg_gpu's path), per step and worker all "
+                                       f"pairs of a run of consecutive anchors at a pair-weighted random SNP "
+                                       f"of the full workload (every distance), {cores} workers, "
                                        f"~{per_step:.0f} s per step"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
