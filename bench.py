@@ -13,8 +13,11 @@ replicates.  ``value`` has inputs resident in HBM; ``e2e`` copies the inputs fro
 pinned host memory and the results back every step.  ``--impl reference`` times the
 CPU restatement of pg_gpu's path (the oracle) on the host cores instead.
 
-Multi-GPU (torchrun): weak scaling, each rank parses its own independently seeded
-workload of the same shape; no data-path collective.
+Multi-GPU (torchrun): weak scaling by default, each rank parses its own independently
+seeded workload of the same shape; no data-path collective.  ``--split``: strong scaling of
+one workload, cut into contiguous anchor ranges of equal pair count (``shard.split_anchors``);
+each rank parses its slab (anchors plus the read-only right halo) and one NCCL all-reduce
+per step sums the per-block bin outputs before the bootstrap replicates.
 """
 from __future__ import annotations
 
@@ -224,6 +227,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="call ldk_parse per step instead of a graph replay")
     ap.add_argument("--no-autotune", action="store_true", help="default tile width, no tuning")
+    ap.add_argument("--split", action="store_true",
+                    help="strong scaling: one workload split into anchor ranges over the ranks")
     ap.add_argument("--all-pairs", action="store_true",
                     help="time the all-pairs LD kernel (ldk_ld_matrix) instead of the binned parse")
     ap.add_argument("--snps", type=int, default=24576, help="--all-pairs: SNPs in the set")
@@ -249,18 +254,31 @@ def main():
     from pg_gpu_b200 import _lib, parse, synth
 
     lib = _lib.load()
-    w = make_workload(args.config, args.scale, rank)
+    w = make_workload(args.config, args.scale, 0 if args.split else rank)
     n_pairs = synth.count_pairs(w)
-
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = run_cpu_sample(w, args.cpu_seconds)
+    whole_pairs = n_pairs
+    if args.split:  # this rank's slab: anchors plus the right halo
+        from pg_gpu_b200 import shard
+        wo = [0, w.n_var] if w.window_offsets is None else list(w.window_offsets)
+        seg = shard.split_anchors(w.positions, wo, w.max_dist, ws, align=_lib.tc_row_blocks(w.genotypes)[0])[rank]
+        w = shard.slab_workload(w, seg)
+        n_pairs = synth.count_pairs(w)
+    split_comm = args.split and ws > 1
+
+    def combine(out):
+        """Sum the ranks' per-block outputs (the split's one collective)."""
+        if split_comm:
+            for t in (out.sums, out.r2_sums, out.pairs, out.r2_counts):
+                dist.all_reduce(t, op=dist.ReduceOp.SUM)
 
     if not args.no_autotune:
         _lib.autotune(True)
     parser = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, genotypes=w.genotypes, method=args.method,
                           max_dist=w.max_dist, window_offsets=w.window_offsets, snp_block=w.snp_block,
-                          n_blocks=w.n_blocks, device=dev)
+                          n_blocks=w.n_blocks, anchor_end=w.anchor_end, device=dev)
     reps_w = torch.as_tensor(w.replicate_weights if w.replicate_weights is not None
                              else np.ones((1, w.n_blocks), np.int32), dtype=torch.int32, device=dev)
     if w.window_of_block is not None:
@@ -285,9 +303,17 @@ def main():
     if args.no_graph:
         def step():
             r = parser.run()
+            combine(r)
             reps = parse.block_combine(r.sums, reps_w)
             wins = parse.block_combine(r.sums, win_w)
             return r, reps, wins
+    elif split_comm:  # the parse replayed as a graph; the all-reduce and replicates after it
+        graph, _ = parser.graph()
+
+        def step():
+            graph.replay()
+            combine(parser.out)
+            return parser.out, parse.block_combine(parser.out.sums, reps_w), parse.block_combine(parser.out.sums, win_w)
     else:
         graph, (g_reps, g_wins) = parser.graph(
             after=lambda out: (parse.block_combine(out.sums, reps_w), parse.block_combine(out.sums, win_w)))
@@ -321,7 +347,7 @@ def main():
         t = torch.tensor([elapsed_ms], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_max = float(t.item())
-    total_pairs = n_pairs * args.steps * ws
+    total_pairs = (whole_pairs if args.split else n_pairs * ws) * args.steps
     value = total_pairs / (t_max / 1e3)
     ms_per_step = t_max / args.steps
     if not args.no_graph:
@@ -349,7 +375,7 @@ def main():
     if parser.block is not None:
         h_in["block"] = blk_h
     h2d = sum(t.numel() * t.element_size() for t in h_in.values())
-    if args.no_graph:
+    if args.no_graph or split_comm:  # steps in series on one stream
         outs_h = [host_outputs()]
 
         def e2e_step(k):
@@ -368,7 +394,7 @@ def main():
         def make_slot():
             p = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, genotypes=w.genotypes, method=args.method,
                              max_dist=w.max_dist, window_offsets=w.window_offsets, snp_block=w.snp_block,
-                             n_blocks=w.n_blocks, device=dev)
+                             n_blocks=w.n_blocks, anchor_end=w.anchor_end, device=dev)
             rw = torch.empty_like(reps_w)
             rw.copy_(reps_w)
             ins = {"X": p.X, "pos": p.pos, "block": p.block, "reps_w": rw}
@@ -396,7 +422,7 @@ def main():
     e2e_done()
     f1.record(stream)
     torch.cuda.synchronize()
-    if not args.no_graph:
+    if not (args.no_graph or split_comm):
         pipe.status()
         # the last step's results, copied out through the pipeline, match the resident run
         last = outs_h[(args.steps - 1) % 2]
@@ -417,7 +443,7 @@ def main():
         fast = {k: v.copy() for k, v in parser.out.numpy().items()}
         pp = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, genotypes=w.genotypes, method="plain",
                           max_dist=w.max_dist, window_offsets=w.window_offsets, snp_block=w.snp_block,
-                          n_blocks=w.n_blocks, device=dev)
+                          n_blocks=w.n_blocks, anchor_end=w.anchor_end, device=dev)
         pp.run()
         torch.cuda.synchronize()
         if ws > 1:
@@ -435,6 +461,7 @@ def main():
             t = torch.tensor([pms], device=dev, dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             pms = float(t.item())
+        combine(pp.out)  # a split compares the combined outputs
         ref = pp.out.numpy()
         tot_f, tot_p = fast["sums"].sum(axis=0), ref["sums"].sum(axis=0)
         parity = {
@@ -445,7 +472,7 @@ def main():
                                                       / np.maximum(np.abs(ref["sums"]), 1e-300))),
             "reference": "plain FP64 kernel, same workload",
         }
-        plain = {"value": n_pairs * ws / (pms / 1e3), "ms_per_step": pms,
+        plain = {"value": (whole_pairs if args.split else n_pairs * ws) / (pms / 1e3), "ms_per_step": pms,
                  "kernel_ms": statistics.mean(pk) if pk else None}
         del pp
 
@@ -485,7 +512,7 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None,
+            "scaling": "strong" if args.split else "weak", "vs_baseline": None,
             "dtype": {"tc": "u8 counts / s32 accumulate / f64 estimators",
                       "plain": "i8 byte counts / f64 estimators"}[args.method],
             "data": "synthetic (seeded founder mosaics; no public dataset offline)",
@@ -496,7 +523,11 @@ def main():
                        int(len(w.window_offsets) - 1) if w.window_offsets is not None else 1,
                        "bootstrap_blocks": int(w.n_blocks),
                        "bootstrap_replicates": int(reps_w.shape[0]),
-                       "method": args.method, "parallelism": f"weak x{ws}, no data-path collective",
+                       "method": args.method,
+                       "parallelism": (f"strong x{ws}: anchor ranges with right halo, one all-reduce of the "
+                                       f"per-block bin outputs per step") if args.split
+                       else f"weak x{ws}, no data-path collective",
+                       "whole_workload_pairs": int(whole_pairs),
                        "tile_partners": int(parser.tile_width()),
                        "tile_source": "autotuned (ldk_autotune)" if not args.no_autotune else "default",
                        "l2": "inputs larger than L2 (haplotypes %d MB, indicator planes %d MB)" % (

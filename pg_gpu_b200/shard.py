@@ -116,3 +116,15 @@ def slab_of(segments):
         offs.append(offs[-1] + (h - a))
     snps = np.concatenate(idx) if idx else np.zeros(0, np.int64)
     return snps, np.asarray(offs, dtype=np.int64), np.asarray(ends, dtype=np.int64)
+
+
+def slab_workload(w, segments):
+    """The workload one rank of an anchor split parses: its slab of ``w`` (a
+    ``synth.Workload``) with local window offsets and ``anchor_end``; bootstrap blocks keep
+    their global ids."""
+    import dataclasses
+    snps, offs, ends = slab_of(segments)
+    return dataclasses.replace(
+        w, data=np.ascontiguousarray(w.data[:, snps]), positions=w.positions[snps].copy(),
+        window_offsets=offs, anchor_end=ends,
+        snp_block=None if w.snp_block is None else w.snp_block[snps].copy())

@@ -36,6 +36,7 @@ class Workload:
     replicate_weights: np.ndarray | None = None  # (n_rep, n_blocks) bootstrap multiplicities
     window_of_block: np.ndarray | None = None
     meta: dict = field(default_factory=dict)
+    anchor_end: np.ndarray | None = None  # per window: left SNPs end here (a rank's slab of a split)
 
     @property
     def n_var(self):
@@ -212,8 +213,11 @@ def count_pairs(w: Workload) -> int:
     """Pairs i < j within a window with pos[j] - pos[i] <= max_dist."""
     offs = w.window_offsets if w.window_offsets is not None else np.array([0, w.n_var])
     tot = 0
-    for a, b in zip(offs[:-1], offs[1:]):
+    for k, (a, b) in enumerate(zip(offs[:-1], offs[1:])):
         p = w.positions[a:b]
         jm = np.searchsorted(p, p + w.max_dist, side="right")
-        tot += int(np.sum(np.maximum(0, jm - np.arange(len(p)) - 1)))
+        per = np.maximum(0, jm - np.arange(len(p)) - 1)
+        if w.anchor_end is not None:
+            per = per[:max(0, int(w.anchor_end[k]) - a)]
+        tot += int(np.sum(per))
     return tot
