@@ -227,6 +227,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="call ldk_parse per step instead of a graph replay")
     ap.add_argument("--no-autotune", action="store_true", help="default tile width, no tuning")
+    ap.add_argument("--packed", action="store_true",
+                    help="inputs stored two bits per entry (parse.pack_codes): a quarter of the bytes to copy")
     ap.add_argument("--split", action="store_true",
                     help="strong scaling: one workload split into anchor ranges over the ranks")
     ap.add_argument("--all-pairs", action="store_true",
@@ -276,7 +278,9 @@ def main():
 
     if not args.no_autotune:
         _lib.autotune(True)
-    parser = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, genotypes=w.genotypes, method=args.method,
+    x_in = parse.pack_codes(w.data) if args.packed else w.data  # the input as the host stores it
+    parser = parse.Parser(x_in, w.positions, w.pop_rows, w.edges, genotypes=w.genotypes, method=args.method,
+                          packed=args.packed,
                           max_dist=w.max_dist, window_offsets=w.window_offsets, snp_block=w.snp_block,
                           n_blocks=w.n_blocks, anchor_end=w.anchor_end, device=dev)
     reps_w = torch.as_tensor(w.replicate_weights if w.replicate_weights is not None
@@ -359,7 +363,7 @@ def main():
     # (pinned host -> device) while the previous step parses, and its results copied out
     # while the next one parses; the timed region spans the first copy in to the last copy
     # out.  Without graphs the steps run in series on one stream.
-    X_h = torch.from_numpy(np.ascontiguousarray(w.data)).pin_memory()
+    X_h = torch.from_numpy(np.ascontiguousarray(x_in).view(np.int8)).pin_memory()
     pos_h = torch.from_numpy(np.ascontiguousarray(w.positions)).pin_memory()
     blk_h = torch.from_numpy(np.ascontiguousarray(w.snp_block if w.snp_block is not None
                                                   else np.zeros(w.n_var, np.int32))).pin_memory()
@@ -392,7 +396,8 @@ def main():
             pass
     else:
         def make_slot():
-            p = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, genotypes=w.genotypes, method=args.method,
+            p = parse.Parser(x_in, w.positions, w.pop_rows, w.edges, genotypes=w.genotypes, method=args.method,
+                             packed=args.packed,
                              max_dist=w.max_dist, window_offsets=w.window_offsets, snp_block=w.snp_block,
                              n_blocks=w.n_blocks, anchor_end=w.anchor_end, device=dev)
             rw = torch.empty_like(reps_w)
@@ -524,6 +529,7 @@ def main():
                        "bootstrap_blocks": int(w.n_blocks),
                        "bootstrap_replicates": int(reps_w.shape[0]),
                        "method": args.method,
+                       "input": "2-bit packed codes (LDK_X_PACKED2)" if args.packed else "int8 codes",
                        "parallelism": (f"strong x{ws}: anchor ranges with right halo, one all-reduce of the "
                                        f"per-block bin outputs per step") if args.split
                        else f"weak x{ws}, no data-path collective",

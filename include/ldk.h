@@ -111,7 +111,18 @@ typedef struct {
                                    A rank of a split parse passes its SNP slab -- its anchors and
                                    the read-only right halo of max_dist after them -- as a window
                                    with anchor_end at the end of its anchors. */
+    int32_t x_format;           /* LDK_X_INT8 (0) or LDK_X_PACKED2 (1); see below */
 } ldk_parse_t;
+/* Layouts of ldk_parse_t.X:
+ *  LDK_X_INT8     one int8 code per entry, row stride ld_x >= n_var (pg_gpu's matrix layout,
+ *                 haplotype_matrix.py:34-83, genotype_matrix.py:32-71);
+ *  LDK_X_PACKED2  two bits per entry holding code + 1 (0: missing, 1..3: codes 0..2), four
+ *                 consecutive SNPs of a row per byte, SNP v in bits 2 (v % 4) .. 2 (v % 4) + 1
+ *                 of byte v / 4; ld_x is the row stride in bytes (>= ceil(n_var / 4)).  A
+ *                 quarter of the bytes to move from the host; read by the tensor-core method
+ *                 (the plain method returns LDK_ERR_UNSUPPORTED). */
+#define LDK_X_INT8 0
+#define LDK_X_PACKED2 1
 /* Limits of the tensor-core method (LDK_METHOD_TC), none of which bind
  * LDK_METHOD_PLAIN_FP64:
  *  - each row block -- 64 SNPs (genotypes: 128) counted from each window's first SNP --

@@ -24,6 +24,8 @@ NOALLOC_SCRATCH_BYTES = 64 << 20
 MAX_BINS = 64
 METHOD_PLAIN = 0
 METHOD_TC = 1
+X_INT8 = 0
+X_PACKED2 = 1
 
 c_i8p = ctypes.c_void_p
 c_vp = ctypes.c_void_p
@@ -46,7 +48,7 @@ class ParseDesc(ctypes.Structure):
         ("max_dist", ctypes.c_double), ("n_bins", ctypes.c_int32),
         ("edges", ctypes.c_double * (MAX_BINS + 1)), ("window_offsets", c_vp), ("n_windows", ctypes.c_int32),
         ("snp_block", c_vp), ("n_blocks", ctypes.c_int32), ("method", ctypes.c_int32),
-        ("anchor_end", c_vp),
+        ("anchor_end", c_vp), ("x_format", ctypes.c_int32),
     ]
 
 

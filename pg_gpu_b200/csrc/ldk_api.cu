@@ -144,7 +144,9 @@ int validate(const ldk_parse_t* d) {
         if (!(d->edges[b] < d->edges[b + 1])) { set_error("bin edges must increase"); return LDK_ERR_ARG; }
     if (d->n_var < 0 || d->n_var > (int64_t)INT32_MAX - 1024) { set_error("n_var out of range"); return LDK_ERR_ARG; }
     if (d->n_var > 0 && (!d->X || !d->pos || !d->pop_rows)) { set_error("null input pointer"); return LDK_ERR_ARG; }
-    if (d->ld_x < d->n_var) { set_error("ld_x < n_var"); return LDK_ERR_ARG; }
+    if (d->x_format != LDK_X_INT8 && d->x_format != LDK_X_PACKED2) { set_error("unknown x_format"); return LDK_ERR_ARG; }
+    if (d->x_format == LDK_X_INT8 && d->ld_x < d->n_var) { set_error("ld_x < n_var"); return LDK_ERR_ARG; }
+    if (d->x_format == LDK_X_PACKED2 && d->ld_x < (d->n_var + 3) / 4) { set_error("ld_x < ceil(n_var / 4) packed bytes"); return LDK_ERR_ARG; }
     if (d->pop_offsets[0] != 0) { set_error("pop_offsets[0] must be 0"); return LDK_ERR_ARG; }
     for (int p = 0; p < d->n_pops; ++p)
         if (d->pop_offsets[p + 1] <= d->pop_offsets[p]) { set_error("empty population %d", p); return LDK_ERR_ARG; }
@@ -169,6 +171,10 @@ int validate(const ldk_parse_t* d) {
                 set_error("anchor_end[%d] outside its window", w);
                 return LDK_ERR_ARG;
             }
+    if (d->x_format == LDK_X_PACKED2 && d->method == LDK_METHOD_PLAIN_FP64) {
+        set_error("the plain method reads int8 codes; packed input needs LDK_METHOD_TC");
+        return LDK_ERR_UNSUPPORTED;
+    }
     return LDK_OK;
 }
 

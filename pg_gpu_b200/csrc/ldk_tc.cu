@@ -23,7 +23,7 @@ struct PrepArgs {
     int planes;
     uint8_t* planes_out;
     unsigned* status;
-};
+};  // X: int8 codes, or (PACKED) 2-bit codes + 1, four SNPs per byte (LDK_X_PACKED2)
 
 constexpr int kPrepV = 128, kPrepK = 128;
 
@@ -35,8 +35,10 @@ constexpr int kPrepV = 128, kPrepK = 128;
 //   haplotypes  h = [x == 1], v = [x in {0, 1}]
 //   genotypes   [x == 1], [x == 2], [x in {0, 1, 2}], 0
 // Padding (127) and invalid codes give 0 in every plane; invalid codes also raise
-// LDK_DEVERR_BAD_INPUT.
-template <bool GENO>
+// LDK_DEVERR_BAD_INPUT.  PACKED: X holds 2-bit fields (code + 1), SNP v in bits 2 (v % 4) of
+// byte v / 4 of its row; four neighbouring threads read the same byte and each unpacks its
+// own field, so the gather moves a quarter of the bytes.
+template <bool GENO, bool PACKED>
 __global__ void __launch_bounds__(256) k_prep_planes(PrepArgs a) {
     constexpr int PL = GENO ? 4 : 2;
     constexpr int RS = kPrepK + 4;  // bytes per SNP row: 33 words, so both the gather's byte
@@ -66,14 +68,18 @@ __global__ void __launch_bounds__(256) k_prep_planes(PrepArgs a) {
         const int vv = threadIdx.x % kPrepV, kb = threadIdx.x / kPrepV;
         const int64_t v = v0 + vv;
         const bool vin = v < a.n_var;
-        const int8_t* col = a.X + v;
+        const int8_t* col = a.X + (PACKED ? (v >> 2) : v);
+        const int shift = 2 * (int)(v & 3);
         int8_t* trow = tile + vv * RS;
 #pragma unroll 16
         for (int kk = kb; kk < kPrepK; kk += kRowStep) {
             const int row = srow[kk];
             int8_t x = 127;
             if (row >= 0 && vin) {
-                x = __ldg(col + (int64_t)row * a.ld);
+                if constexpr (PACKED)
+                    x = (int8_t)((((unsigned)(uint8_t)__ldg(col + (int64_t)row * a.ld)) >> shift & 3u) - 1u);
+                else
+                    x = __ldg(col + (int64_t)row * a.ld);
                 bad |= (x < -1 || x > xmax);
             }
             trow[kk] = x;
@@ -233,8 +239,14 @@ cudaError_t launch_prep_planes(const ldk_parse_t* d, const Scratch& w, const Par
     a.planes_out = w.hv;
     a.status = w.status;
     dim3 grid((unsigned)((d->n_var + kPrepV - 1) / kPrepV), (unsigned)(sh.ktot / kPrepK));
-    if (sh.genotypes) k_prep_planes<true><<<grid, 256, 0, s>>>(a);
-    else k_prep_planes<false><<<grid, 256, 0, s>>>(a);
+    const bool packed = d->x_format == LDK_X_PACKED2;
+    if (sh.genotypes) {
+        if (packed) k_prep_planes<true, true><<<grid, 256, 0, s>>>(a);
+        else k_prep_planes<true, false><<<grid, 256, 0, s>>>(a);
+    } else {
+        if (packed) k_prep_planes<false, true><<<grid, 256, 0, s>>>(a);
+        else k_prep_planes<false, false><<<grid, 256, 0, s>>>(a);
+    }
     return cudaGetLastError();
 }
 

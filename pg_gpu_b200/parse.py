@@ -13,7 +13,9 @@ finite r^2.  Two counting/estimator methods:
   block may span at most two (four) bootstrap blocks).  Both are GPU kernels.
 
 ``Pipeline`` runs a stream of same-shape parses from pinned host memory with the copies
-overlapped with the parses.
+overlapped with the parses.  ``pack_codes`` stores a matrix in two bits per entry
+(``ldk_parse_t.x_format = LDK_X_PACKED2``), a quarter of the bytes to copy to the GPU;
+``Parser(..., packed=True)`` parses it (tensor-core method).
 """
 from __future__ import annotations
 
@@ -62,6 +64,28 @@ def tc_blocks_fit(snp_block, window_offsets, n_var, genotypes=False) -> bool:
     return True
 
 
+def pack_codes(data):
+    """(n_rows, n_var) int8 codes in {-1, 0, 1, 2} -> (n_rows, ceil(n_var / 4)) uint8: each
+    entry as code + 1 in two bits, SNP v in bits 2 (v % 4) of byte v / 4 (LDK_X_PACKED2)."""
+    x = np.asarray(data)
+    if x.ndim != 2:
+        raise ValueError("data must be (n_rows, n_var)")
+    if x.size and (x.min() < -1 or x.max() > 2):
+        raise ValueError("codes must lie in {-1, 0, 1, 2}")
+    n_rows, n_var = x.shape
+    c = np.zeros((n_rows, (n_var + 3) // 4 * 4), np.uint8)
+    c[:, :n_var] = (x.astype(np.int16) + 1).astype(np.uint8)
+    c = c.reshape(n_rows, -1, 4)
+    return np.ascontiguousarray(c[..., 0] | (c[..., 1] << 2) | (c[..., 2] << 4) | (c[..., 3] << 6))
+
+
+def unpack_codes(packed, n_var):
+    """Inverse of ``pack_codes``."""
+    p = np.asarray(packed, dtype=np.uint8)
+    c = np.stack([(p >> s) & 3 for s in (0, 2, 4, 6)], axis=-1).reshape(p.shape[0], -1)
+    return (c[:, :n_var].astype(np.int16) - 1).astype(np.int8)
+
+
 def _dev(x, dtype, torch, device):
     if isinstance(x, torch.Tensor):
         t = x.to(device=device, dtype=dtype)
@@ -75,16 +99,26 @@ class Parser:
     that repeated calls allocate nothing (the CUDA library itself never allocates)."""
 
     def __init__(self, data, positions, pop_rows, edges, *, genotypes=False, method="auto", max_dist=None,
-                 coords=None, window_offsets=None, snp_block=None, n_blocks=1, anchor_end=None, device=None):
+                 coords=None, window_offsets=None, snp_block=None, n_blocks=1, anchor_end=None, packed=False,
+                 device=None):
         torch = _lib.require_cuda()
         lib = _lib.load()
         device = torch.device(device or "cuda")
         self.torch = torch
         self.lib = lib
-        self.X = _dev(data, torch.int8, torch, device)
-        if self.X.dim() != 2:
-            raise ValueError("data must be (n_rows, n_var)")
-        n_rows, n_var = self.X.shape
+        if packed:  # pack_codes output: the SNP count comes from the positions
+            self.X = _dev(data.view(torch.int8) if isinstance(data, torch.Tensor) else np.asarray(data).view(np.int8),
+                          torch.int8, torch, device)
+            if self.X.dim() != 2:
+                raise ValueError("packed data must be (n_rows, ceil(n_var / 4))")
+            n_rows, n_var = self.X.shape[0], len(positions)
+            if self.X.shape[1] < (n_var + 3) // 4:
+                raise ValueError("packed data holds fewer SNPs than the positions")
+        else:
+            self.X = _dev(data, torch.int8, torch, device)
+            if self.X.dim() != 2:
+                raise ValueError("data must be (n_rows, n_var)")
+            n_rows, n_var = self.X.shape
         P = len(pop_rows)
         if not 1 <= P <= _lib.MAX_POPS:
             raise ValueError("1-4 populations supported")
@@ -110,7 +144,8 @@ class Parser:
                                                          torch.int32, torch, device)
         d = _lib.ParseDesc()
         d.X = _lib.ptr(self.X)
-        d.ld_x = n_var
+        d.ld_x = self.X.shape[1]
+        d.x_format = _lib.X_PACKED2 if packed else _lib.X_INT8
         d.n_rows = n_rows
         d.n_var = n_var
         d.genotypes = int(bool(genotypes))

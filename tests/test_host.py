@@ -109,3 +109,17 @@ def test_genotype_horner_forms_are_exact_in_fp64():
         want = eval(poly, {}, {"x": x})
         got = eval(G.horner_form(poly), {}, {"x": x})
         np.testing.assert_array_equal(got, want)
+
+
+def test_pack_codes_round_trip():
+    """Two-bit packing of the ingest layout (LDK_X_PACKED2): code + 1 in bits 2 (v % 4) of
+    byte v / 4; unpacking restores every code, at every n_var modulo 4."""
+    from pg_gpu_b200 import parse
+    rng = np.random.default_rng(7)
+    for n_var in (1, 2, 3, 4, 5, 130):
+        x = rng.integers(-1, 3, size=(9, n_var)).astype(np.int8)
+        p = parse.pack_codes(x)
+        assert p.dtype == np.uint8 and p.shape == (9, (n_var + 3) // 4)
+        np.testing.assert_array_equal(parse.unpack_codes(p, n_var), x)
+        v = n_var - 1
+        np.testing.assert_array_equal((p[:, v // 4] >> (2 * (v % 4))) & 3, x[:, v] + 1)
