@@ -481,6 +481,17 @@ def main():
                  "kernel_ms": statistics.mean(pk) if pk else None}
         del pp
 
+    # ---- the tuning table's choice for this shape (tile width, row-block order)
+    tuned_entry = None
+    if not args.no_autotune and args.method == "tc":
+        with tempfile.TemporaryDirectory() as td:
+            tp = os.path.join(td, "tune.json")
+            if _lib.autotune_save(tp) > 0:
+                ents = json.load(open(tp))["entries"]
+                mine = [e for e in ents if e["pops"] == len(w.pop_rows) and e["genotypes"] == int(w.genotypes)
+                        and e["bins"] == len(w.edges) - 1]
+                tuned_entry = mine[0] if len(mine) == 1 else None
+
     # ---- roofline of the dominant kernel
     pk_d, pk_kind = peaks()
     probe_i8, probe_f64 = _lib.probe_peaks()
@@ -536,6 +547,7 @@ def main():
                        "whole_workload_pairs": int(whole_pairs),
                        "tile_partners": int(parser.tile_width()),
                        "tile_source": "autotuned (ldk_autotune)" if not args.no_autotune else "default",
+                       "tuned": tuned_entry,
                        "l2": "inputs larger than L2 (haplotypes %d MB, indicator planes %d MB)" % (
                            w.data.nbytes >> 20, (w.n_var * 2 * parser_ktot(w)) >> 20)},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},

@@ -214,18 +214,36 @@ LDK_API int ldk_ld_matrix(const int8_t* X, int64_t ld_x, int64_t n_var, const in
                           int estimator, double* out, int64_t ld_out, double* sums, void* workspace,
                           size_t workspace_bytes, void* stream);
 
-/* Tile autotuning of the tensor-core parse.  No counterpart in pg_gpu.  With enable = 1
- * (or LDK_AUTOTUNE=1 in the environment at the first call), the first ldk_parse of each
- * shape (population count, haplotype or genotype path, method, padded sample count) runs
- * every candidate partner-tile width twice on its own input, times the second run of each
- * with CUDA events,
- * and keeps the fastest in a process-wide table (behind a mutex); that call then clears
- * its outputs and runs the kept width on its input.  Later ldk_parse and
- * ldk_parse_enqueue calls of the shape use the kept width; shapes never tuned use the
- * default width.  ldk_tile_width returns the width (SNPs per partner tile) a call with
- * this descriptor would use now, 0 for the plain method, or a negative status. */
+/* Autotuning of the tensor-core parse.  Replaces the memory-driven pair-chunk sizing of
+ * ld_pipeline.estimate_ld_chunk_size (ld_pipeline.py:16-49): the work here is a fixed tile
+ * schedule, and the tuner picks among its variants.  With enable = 1 (or LDK_AUTOTUNE=1 in
+ * the environment at the first call), the first ldk_parse of each shape class runs every
+ * candidate -- partner-tile width (two widths per population count and path) x row-block
+ * claim order (largest windows first, or window order; several windows only) -- twice on
+ * its own input, times the second run of each with CUDA events, and keeps the fastest in a
+ * process-wide table behind a mutex; that call then clears its outputs and runs the kept
+ * candidate.  A shape class is (population count, haplotype or genotype path, padded sample
+ * bytes, bin count, decade of max_dist, log2 of the mean window size).  Later ldk_parse,
+ * ldk_parse_setup (the order) and ldk_parse_enqueue (the width) calls of the class use the
+ * kept choice, tuning enabled or not; classes never tuned use the defaults (widest tile,
+ * largest windows first).  ldk_tile_width returns the width (SNPs per partner tile) a call
+ * with this descriptor would use now, 0 for the plain method, or a negative status.  No
+ * counterpart in pg_gpu. */
 LDK_API int ldk_autotune(int enable);
 LDK_API int ldk_tile_width(const ldk_parse_t* d);
+
+/* The tuning table as a JSON file ({"format": "ldk-autotune", "version": 1, "entries":
+ * [...]}, one entry per shape class with its choice and time).  ldk_autotune_load merges a
+ * file into the table (returns the entries read, or LDK_ERR_ARG if the file is not such a
+ * table); ldk_autotune_save writes the whole table (returns the entries written).  With
+ * LDK_AUTOTUNE_CACHE=<path> in the environment the file is loaded at the first lookup and
+ * rewritten after every tuning, so a later process starts from it without re-tuning.
+ * ldk_autotune_count returns the table's size and, in *tunings (may be NULL), how many
+ * tunings this process ran; ldk_autotune_clear empties the table.  Host-only. */
+LDK_API int ldk_autotune_load(const char* path);
+LDK_API int ldk_autotune_save(const char* path);
+LDK_API int ldk_autotune_count(int* tunings);
+LDK_API int ldk_autotune_clear(void);
 
 /* Row blocks of the tensor-core methods (genotypes 0: haplotype path, 1: genotype path):
  * *rows SNPs per row block, counted from each window's first SNP, and *max_blocks, the

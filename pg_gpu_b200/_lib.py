@@ -82,6 +82,10 @@ EXPORTS = {
     "ldk_ld_matrix": (ctypes.c_int, [c_vp, ctypes.c_int64, ctypes.c_int64, c_vp, ctypes.c_int32, ctypes.c_int, c_vp,
                                      ctypes.c_int64, c_vp, c_vp, ctypes.c_size_t, c_vp]),
     "ldk_tile_width": (ctypes.c_int, [ctypes.POINTER(ParseDesc)]),
+    "ldk_autotune_load": (ctypes.c_int, [ctypes.c_char_p]),
+    "ldk_autotune_save": (ctypes.c_int, [ctypes.c_char_p]),
+    "ldk_autotune_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
+    "ldk_autotune_clear": (ctypes.c_int, []),
     "ldk_tc_row_blocks": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]),
     "ldk_profile": (ctypes.c_int, [ctypes.c_int]),
     "ldk_profile_last_kernel_ms": (ctypes.c_double, []),
@@ -151,6 +155,33 @@ def probe_peaks(stream=None):
 def autotune(enable=True):
     """Turn tile autotuning of the tensor-core parse on or off (``ldk_autotune``)."""
     check(load().ldk_autotune(int(bool(enable))))
+
+
+def autotune_load(path):
+    """Merge a saved tuning table (JSON) into the process table; returns its entries."""
+    n = load().ldk_autotune_load(os.fsencode(path))
+    if n < 0:
+        check(n)
+    return n
+
+
+def autotune_save(path):
+    """Write the process tuning table as JSON; returns the entries written."""
+    n = load().ldk_autotune_save(os.fsencode(path))
+    if n < 0:
+        check(n)
+    return n
+
+
+def autotune_count():
+    """(entries in the tuning table, tunings this process ran)."""
+    t = ctypes.c_int()
+    n = load().ldk_autotune_count(ctypes.byref(t))
+    return n, t.value
+
+
+def autotune_clear():
+    check(load().ldk_autotune_clear())
 
 
 def tc_row_blocks(genotypes: bool):

@@ -251,10 +251,37 @@ int check_outputs(const ldk_parse_out_t* out) {
     return LDK_OK;
 }
 
+// The tensor-core row-block list (64 SNPs for haplotypes, 128 for genotypes, up to each
+// window's anchor end) in claim order: 0 = the largest windows' row blocks first, 1 = window
+// order.  The kernel's CTAs claim row blocks in list order.
+int upload_items(const ldk_parse_t* d, const Prepared& P, cudaStream_t s, int claim_order) {
+    int rc;
+    const int rows = tc_rows_per_block(P.sh);
+    std::vector<int> order(window_count(d));
+    for (int k = 0; k < (int)order.size(); ++k) order[k] = k;
+    if (claim_order == 0)
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+            return (window_bound(d, x + 1) - window_bound(d, x)) > (window_bound(d, y + 1) - window_bound(d, y));
+        });
+    std::vector<int32_t> items;
+    items.reserve((size_t)P.L.n_items * 2);
+    for (int wi : order) {
+        const int64_t ae = anchor_bound(d, wi);
+        for (int64_t r0 = window_bound(d, wi); r0 < ae; r0 += rows) {
+            items.push_back((int32_t)r0);
+            items.push_back((int32_t)std::min<int64_t>(r0 + rows, ae));
+        }
+    }
+    if (!items.empty() &&
+        (rc = check_cuda(cudaMemcpyAsync(P.w.items, items.data(), items.size() * sizeof(int32_t),
+                                         cudaMemcpyHostToDevice, s), "upload row blocks")))
+        return rc;
+    return LDK_OK;
+}
+
 // Host-side plan into the workspace: window offsets and, for the tensor-core method, the
-// row-block list (64 SNPs for haplotypes, 128 for genotypes, largest windows first; the
-// kernel's CTAs claim them in this order) -- or, with device_items, the list is built on
-// the device in window order.
+// row-block list in the tuned claim order (largest windows first if the shape is untuned)
+// -- or, with device_items, the list is built on the device in window order.
 int upload_plan(const ldk_parse_t* d, const Prepared& P, cudaStream_t s, bool device_items) {
     int rc;
     const int nw = window_count(d);
@@ -265,28 +292,10 @@ int upload_plan(const ldk_parse_t* d, const Prepared& P, cudaStream_t s, bool de
                                          cudaMemcpyHostToDevice, s), "upload windows")))
         return rc;
     if (d->method == LDK_METHOD_PLAIN_FP64) return LDK_OK;
-    const int rows = tc_rows_per_block(P.sh);
     if (device_items)
-        return check_cuda(launch_build_items(P.w, window_count(d), rows, s), "row blocks");
-    std::vector<int> order(window_count(d));
-    for (int k = 0; k < (int)order.size(); ++k) order[k] = k;
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-        return (woff[x + 1] - woff[x]) > (woff[y + 1] - woff[y]);
-    });
-    std::vector<int32_t> items;
-    items.reserve((size_t)P.L.n_items * 2);
-    for (int wi : order) {
-        const int64_t ae = anchor_bound(d, wi);
-        for (int64_t r0 = woff[wi]; r0 < ae; r0 += rows) {
-            items.push_back((int32_t)r0);
-            items.push_back((int32_t)std::min<int64_t>(r0 + rows, ae));
-        }
-    }
-    if (!items.empty() &&
-        (rc = check_cuda(cudaMemcpyAsync(P.w.items, items.data(), items.size() * sizeof(int32_t),
-                                         cudaMemcpyHostToDevice, s), "upload row blocks")))
-        return rc;
-    return LDK_OK;
+        return check_cuda(launch_build_items(P.w, window_count(d), tc_rows_per_block(P.sh), s), "row blocks");
+    TuneChoice c;
+    return upload_items(d, P, s, tune_lookup(tune_key_of(d, P.sh), &c) ? c.order : 0);
 }
 
 // Zeroes the outputs, the status block and the fixed-point bin accumulators.
@@ -305,10 +314,8 @@ int clear(const ldk_parse_t* d, const ldk_parse_out_t* out, const Prepared& P, c
 
 // Device work of one parse (after the plan is in the workspace): pair ranges, indicator
 // planes and the parse kernel.  Host work: tensor-map encoding and launch configuration.
-// ---- tile autotuning: the fastest tile variant per shape, process-wide behind a mutex
+// ---- autotuning: the fastest (tile variant, row-block order) per shape class (ldk_tune.cu)
 std::atomic<int> g_autotune{-1};  // -1: LDK_AUTOTUNE not read yet
-std::mutex g_tune_mu;
-std::map<std::array<int, 4>, int> g_tuned;  // (populations, genotypes, method, K bytes) -> variant
 
 bool autotune_on() {
     if (g_autotune.load() < 0) {
@@ -319,26 +326,23 @@ bool autotune_on() {
     return g_autotune.load() == 1;
 }
 
-std::array<int, 4> tune_key(const ldk_parse_t* d, const ParseShape& sh) {
-    return {sh.P, sh.genotypes, d->method, sh.ktot};
-}
-
-// The cached variant of this shape; -1 if the shape has not been tuned.
+// The tuned tile variant of this shape; -1 if the shape has not been tuned.
 int tuned_variant(const ldk_parse_t* d, const ParseShape& sh) {
-    std::lock_guard<std::mutex> lock(g_tune_mu);
-    auto it = g_tuned.find(tune_key(d, sh));
-    return it == g_tuned.end() ? -1 : it->second;
+    TuneChoice c;
+    return tune_lookup(tune_key_of(d, sh), &c) ? c.variant : -1;
 }
 
-// Tile variants worth timing: the alternative only where its width differs (the FP32
-// estimators have one variant).
+// Candidates worth timing: the alternative tile only where its width differs, the window
+// order only where there are several windows.
 int n_variants(const ldk_parse_t* d, const ParseShape& sh) {
     return tc_tile_width(sh, 1) != tc_tile_width(sh, 0) ? 2 : 1;
 }
+int n_orders(const ldk_parse_t* d) { return window_count(d) > 1 ? 2 : 1; }
 
-// Runs every tile variant twice on this call's input (outputs cleared before each run) and
-// times the second run with CUDA events; caches the fastest.  The outputs keep the last
-// candidate's sums.
+// Runs every (tile variant, row-block order) candidate twice on this call's input (outputs
+// cleared before each run), times the second run with CUDA events and stores the fastest
+// in the table; the row-block list is left in the winner's order.  The outputs keep the
+// last candidate's sums.
 int autotune_tc(const ldk_parse_t* dd, const ldk_parse_out_t* out, const Prepared& P, cudaStream_t s);
 int read_status(const unsigned* status_dev, cudaStream_t s);
 
@@ -357,7 +361,7 @@ int enqueue_device(const ldk_parse_t* d, const ldk_parse_out_t* out, const Prepa
         if ((rc = check_cuda(launch_prep_planes(&dd, P.w, P.sh, s), "indicator planes"))) return rc;
         if (P.w.rtab && (rc = check_cuda(launch_fill_rtab(P.w.rtab, P.sh.max_n, s), "reciprocal table"))) return rc;
         if (P.w.gtab && (rc = check_cuda(launch_fill_gtab(P.w.gtab, P.sh.max_n, s), "reciprocal table"))) return rc;
-        if (tune && n_variants(d, P.sh) > 1 && tuned_variant(d, P.sh) < 0) {
+        if (tune && n_variants(d, P.sh) * n_orders(d) > 1 && tuned_variant(d, P.sh) < 0) {
             if ((rc = autotune_tc(&dd, out, P, s))) return rc;
             // the candidate runs left their sums and a spent row-block counter behind
             if ((rc = clear(&dd, out, P, s))) return rc;
@@ -377,31 +381,42 @@ int autotune_tc(const ldk_parse_t* dd, const ldk_parse_out_t* out, const Prepare
     int rc;
     if ((rc = check_cuda(cudaEventCreate(&e0), "autotune events"))) return rc;
     if ((rc = check_cuda(cudaEventCreate(&e1), "autotune events"))) { cudaEventDestroy(e0); return rc; }
-    float best_ms = 0.f;
-    int best = -1;
-    for (int v = 0; v < n_variants(dd, P.sh) && !rc; ++v) {
-        // an untimed run first (first-launch costs, caches), then the timed one
-        bool fits = true;
-        float ms = 0.f;
-        for (int rep = 0; rep < 2 && fits && !rc; ++rep) {
-            if ((rc = clear(dd, out, P, s))) break;
-            cudaEventRecord(e0, s);
-            if (launch_parse_tc(dd, out, P.w, P.sh, P.L.n_items, v, s) != cudaSuccess) {
-                cudaGetLastError();  // this variant does not fit the shape (e.g. shared memory): skip it
-                fits = false;
-                break;
+    TuneChoice best;
+    bool found = false;
+    int uploaded = -1;
+    for (int o = 0; o < n_orders(dd) && !rc; ++o) {
+        if ((rc = upload_items(dd, P, s, o))) break;
+        uploaded = o;
+        for (int v = 0; v < n_variants(dd, P.sh) && !rc; ++v) {
+            // an untimed run first (first-launch costs, caches), then the timed one
+            bool fits = true;
+            float ms = 0.f;
+            for (int rep = 0; rep < 2 && fits && !rc; ++rep) {
+                if ((rc = clear(dd, out, P, s))) break;
+                cudaEventRecord(e0, s);
+                if (launch_parse_tc(dd, out, P.w, P.sh, P.L.n_items, v, s) != cudaSuccess) {
+                    cudaGetLastError();  // this variant does not fit the shape (e.g. shared memory): skip it
+                    fits = false;
+                    break;
+                }
+                cudaEventRecord(e1, s);
+                if ((rc = read_status(P.w.status, s))) break;
+                cudaEventElapsedTime(&ms, e0, e1);
             }
-            cudaEventRecord(e1, s);
-            if ((rc = read_status(P.w.status, s))) break;
-            cudaEventElapsedTime(&ms, e0, e1);
+            if (fits && !rc && (!found || ms < best.ms)) {
+                best.variant = v;
+                best.order = o;
+                best.ms = ms;
+                found = true;
+            }
         }
-        if (fits && !rc && (best < 0 || ms < best_ms)) { best = v; best_ms = ms; }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc) return rc;
-    std::lock_guard<std::mutex> lock(g_tune_mu);
-    g_tuned[tune_key(dd, P.sh)] = best < 0 ? 0 : best;
+    if (!found) best = TuneChoice{};
+    if (uploaded != best.order && (rc = upload_items(dd, P, s, best.order))) return rc;
+    tune_store(tune_key_of(dd, P.sh), best);
     return LDK_OK;
 }
 

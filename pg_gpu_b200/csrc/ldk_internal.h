@@ -86,6 +86,26 @@ cudaError_t launch_ld_matrix(const int8_t* X, int64_t ld_x, int64_t n_var, const
                              int estimator, double* out, int64_t ld_out, double* sums, unsigned char* ws,
                              unsigned* status, cudaStream_t s);
 
+// autotuning table (ldk_tune.cu): shape class -> (tile variant, row-block order)
+struct TuneKey {
+    int P, genotypes, ktot, n_bins, cutoff_decade, window_log2;
+    bool operator<(const TuneKey& o) const {
+        const int a[6] = {P, genotypes, ktot, n_bins, cutoff_decade, window_log2};
+        const int b[6] = {o.P, o.genotypes, o.ktot, o.n_bins, o.cutoff_decade, o.window_log2};
+        for (int i = 0; i < 6; ++i)
+            if (a[i] != b[i]) return a[i] < b[i];
+        return false;
+    }
+};
+struct TuneChoice {
+    int variant = 0;  // partner-tile variant (tc_tile_width)
+    int order = 0;    // row blocks: 0 = largest windows first, 1 = window order
+    float ms = 0.f;   // the winning candidate's kernel time when tuned
+};
+TuneKey tune_key_of(const ldk_parse_t* d, const ParseShape& sh);
+bool tune_lookup(const TuneKey& k, TuneChoice* c);
+void tune_store(const TuneKey& k, const TuneChoice& c);
+
 // ldk_parse with a caller-provided workspace; device_items lists the tensor-core row
 // blocks with a device kernel (window order) instead of a host-built upload.
 int parse_impl(const ldk_parse_t* d, const ldk_parse_out_t* out, void* workspace, size_t workspace_bytes,

@@ -35,9 +35,10 @@ def test_struct_layout_matches_c():
 #include <stddef.h>
 #include "ldk.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(ldk_parse_t), offsetof(ldk_parse_t, pop_offsets),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(ldk_parse_t), offsetof(ldk_parse_t, pop_offsets),
          offsetof(ldk_parse_t, max_dist), offsetof(ldk_parse_t, edges), offsetof(ldk_parse_t, window_offsets),
-         offsetof(ldk_parse_t, method), sizeof(ldk_parse_out_t), offsetof(ldk_parse_out_t, r2_counts));
+         offsetof(ldk_parse_t, method), offsetof(ldk_parse_t, anchor_end), offsetof(ldk_parse_t, x_format),
+         sizeof(ldk_parse_out_t), offsetof(ldk_parse_out_t, r2_counts));
   return 0;
 }'''
     with tempfile.TemporaryDirectory() as d:
@@ -49,7 +50,8 @@ int main(void) {
     D, O = _lib.ParseDesc, _lib.ParseOut
     import ctypes
     want = [ctypes.sizeof(D), D.pop_offsets.offset, D.max_dist.offset, D.edges.offset,
-            D.window_offsets.offset, D.method.offset, ctypes.sizeof(O), O.r2_counts.offset]
+            D.window_offsets.offset, D.method.offset, D.anchor_end.offset, D.x_format.offset,
+            ctypes.sizeof(O), O.r2_counts.offset]
     assert got == want
 
 
@@ -75,3 +77,35 @@ def test_no_cpu_fallback():
         pytest.skip("GPU present")
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         _lib.require_cuda()
+
+
+def test_autotune_table_file_round_trip(tmp_path):
+    """The tuning table's JSON file (host-only entry points): a written table loads back
+    entry for entry, clearing empties it, and a file that is not such a table is refused."""
+    import json
+    _lib.autotune_clear()
+    assert _lib.autotune_count()[0] == 0
+    src = tmp_path / "table.json"
+    entries = [{"pops": 3, "genotypes": 0, "k_bytes": 512, "bins": 16, "cutoff_decade": 6, "window_log2": 11,
+                "tile_variant": 1, "tile_partners": 16, "order": 1, "ms": 12.5},
+               {"pops": 1, "genotypes": 1, "k_bytes": 512, "bins": 20, "cutoff_decade": 5, "window_log2": 16,
+                "tile_variant": 0, "tile_partners": 16, "order": 0, "ms": 9.0}]
+    src.write_text('{"format": "ldk-autotune", "version": 1, "entries": [\n'
+                   + ",\n".join(json.dumps(e) for e in entries) + "\n]}\n")
+    assert _lib.autotune_load(str(src)) == 2
+    assert _lib.autotune_count()[0] == 2
+    out = tmp_path / "saved.json"
+    assert _lib.autotune_save(str(out)) == 2
+    saved = json.loads(out.read_text())
+    assert saved["format"] == "ldk-autotune"
+    key = lambda e: (e["pops"], e["genotypes"], e["k_bytes"], e["bins"], e["cutoff_decade"], e["window_log2"])  # noqa
+    got = {key(e): (e["tile_variant"], e["order"], e["tile_partners"]) for e in saved["entries"]}
+    assert got == {key(e): (e["tile_variant"], e["order"], e["tile_partners"]) for e in entries}
+    _lib.autotune_clear()
+    assert _lib.autotune_count()[0] == 0
+    bad = tmp_path / "bad.json"
+    bad.write_text('{"something": "else"}')
+    with pytest.raises(_lib.LdkError):
+        _lib.autotune_load(str(bad))
+    with pytest.raises(_lib.LdkError):
+        _lib.autotune_load(str(tmp_path / "missing.json"))
