@@ -10,8 +10,10 @@ Seeded synthetic data (founder mosaics, see pg_gpu_b200/synth.py).
 One step = the whole batched parse of that workload: pair ranges, indicator planes,
 the fused INT8 tcgen05 count + estimator + bin kernel, per-window totals and bootstrap
 replicates.  ``value`` has inputs resident in HBM; ``e2e`` copies the inputs from
-pinned host memory and the results back every step.  ``--impl reference`` times the
-CPU restatement of pg_gpu's path (the oracle) on the host cores instead.
+pinned host memory and the results back every step.  ``--impl reference`` times pg_gpu's
+path on the host cores instead: its own estimator kernels compiled for the host
+(``oracle/_ref``, haplotype path with one, three or four populations) or the oracle's
+restatement of it.
 
 Multi-GPU (torchrun): weak scaling by default, each rank parses its own independently
 seeded workload of the same shape; no data-path collective.  ``--split``: strong scaling of
@@ -118,12 +120,32 @@ class ClockSampler:
 # CPU side: the oracle (pg_gpu's algorithm restated in NumPy) on a bounded sample
 # ---------------------------------------------------------------------------
 
+CPU_WHAT = {
+    "reference": "pg_gpu's own estimator kernels, compiled for the host from its source (oracle/_ref) and "
+                 "driven by the oracle's restatement of its dispatch; counts and binning as its NumPy code",
+    "port": "the oracle, a NumPy restatement of pg_gpu's path",
+}
+
+
+def cpu_kind(w):
+    """"reference" where pg_gpu's own estimator kernels run on the host (oracle/_ref, built
+    from its source; its kernel path: haplotypes with one, three or four populations),
+    else "port" (the oracle's NumPy restatement)."""
+    from oracle import ref_kernels
+    return "reference" if (not w.genotypes and len(w.pop_rows) != 2 and ref_kernels.available()) else "port"
+
+
 def _cpu_task(args):
-    data, pos, pop_rows, edges, max_dist, n_anchor, genotypes = args
+    data, pos, pop_rows, edges, max_dist, n_anchor, genotypes, kind = args
     os.environ.setdefault("OMP_NUM_THREADS", "1")
     from oracle import ld_oracle as O
+    stat_fn = None
+    if kind == "reference":
+        from oracle import ref_kernels
+        stat_fn = ref_kernels.hap_stats
     t0 = time.perf_counter()
-    r = O.bin_sums(data, pos, pop_rows, edges, genotypes=genotypes, max_dist=max_dist, anchor_end=[n_anchor])
+    r = O.bin_sums(data, pos, pop_rows, edges, genotypes=genotypes, max_dist=max_dist, anchor_end=[n_anchor],
+                   stat_fn=stat_fn)
     return r["n_pairs"], time.perf_counter() - t0
 
 
@@ -140,6 +162,7 @@ def cpu_sample_tasks(w, workers, pairs_per_worker, seed=0):
     for k, (a, b) in enumerate(zip(offs[:-1], offs[1:])):
         win[a:b] = k
     rng = np.random.default_rng(seed)
+    kind = cpu_kind(w)
     tasks = []
     for _ in range(workers):
         a = int(rng.choice(w.n_var, p=per / per.sum()))
@@ -150,7 +173,7 @@ def cpu_sample_tasks(w, workers, pairs_per_worker, seed=0):
             e += 1
         h = max(e, int(jmax[e - 1]))
         tasks.append((np.ascontiguousarray(w.data[:, a:h]), w.positions[a:h].copy(), w.pop_rows, w.edges,
-                      w.max_dist, e - a, bool(w.genotypes)))
+                      w.max_dist, e - a, bool(w.genotypes), kind))
     return tasks
 
 
@@ -193,7 +216,7 @@ def run_cpu_sample(w, seconds, workers=None, pool=None, seed=0):
         pool.join()
     pairs = sum(r[0] for r in res)
     return {"value": pairs / wall, "pairs": pairs, "wall_s": wall, "workers": workers,
-            "per_worker_pairs": per_worker}
+            "per_worker_pairs": per_worker, "kind": tasks[0][-1]}
 
 
 # ---------------------------------------------------------------------------
@@ -567,9 +590,9 @@ def main():
         if parity:
             line["parity"] = parity
         if cpu:
-            line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["workers"], "kind": "port",
+            line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["workers"], "kind": cpu["kind"],
                                     "extrapolated": True,
-                                    "sample": f"oracle (NumPy restatement of pg_gpu's path): per worker all pairs "
+                                    "sample": f"{CPU_WHAT[cpu['kind']]}: per worker all pairs "
                                               f"of ~{cpu['per_worker_pairs']} consecutive-anchor pairs (every "
                                               f"distance) at a pair-weighted random SNP of the full workload, "
                                               f"{cpu['workers']} spawn workers, {cpu['wall_s']:.1f} s wall; the "
@@ -651,7 +674,8 @@ def parser_ktot(w):
 
 
 def run_reference(args, ws, rank):
-    """pg_gpu's path restated on the CPU (the oracle), all host cores, bounded samples."""
+    """pg_gpu's path on the CPU -- its own estimator kernels compiled for the host where they
+    cover the workload, else the oracle's restatement -- all host cores, bounded samples."""
     if ws > 1 and rank != 0:
         return
     w = make_workload(args.config, args.scale, 0)
@@ -662,6 +686,7 @@ def run_reference(args, ws, rank):
     for k in range(max(0, min(args.warmup, 1))):
         run_cpu_sample(w, 1.0, cores, pool, seed=100 + k)
     vals, pairs, wall = [], 0, 0.0
+    kind = cpu_kind(w)
     for k in range(args.steps):
         r = run_cpu_sample(w, per_step, cores, pool, seed=k)
         vals.append(r["value"])
@@ -674,8 +699,8 @@ def run_reference(args, ws, rank):
             "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded founder mosaics)",
             "config": {"workload": w.name, "config_index": args.config, "scale": args.scale},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "extrapolated": True,
-                             "sample": f"oracle (NumPy restatement of pg_gpu's path), per step and worker all "
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "extrapolated": True,
+                             "sample": f"{CPU_WHAT[kind]}; per step and worker all "
                                        f"pairs of a run of consecutive anchors at a pair-weighted random SNP "
                                        f"of the full workload (every distance), {cores} workers, "
                                        f"~{per_step:.0f} s per step"},

@@ -718,7 +718,7 @@ def geno_dosage_r2(counts9):
 
 def bin_sums(data, positions, pop_rows, edges, genotypes=False, chunk=200_000,
              max_dist=None, coords=None, pair_range=None, window_offsets=None,
-             snp_block=None, n_blocks=1, anchor_end=None):
+             snp_block=None, n_blocks=1, anchor_end=None, stat_fn=None):
     """Per-bin sums of the moments-ordered statistics.
 
     Returns dict: ``sums`` (n_blocks, n_bins, n_stats), ``pairs`` (n_blocks, n_bins)
@@ -732,6 +732,8 @@ def bin_sums(data, positions, pop_rows, edges, genotypes=False, chunk=200_000,
     positions and ``max_dist``.  ``pair_range`` = (lo, hi) restricts to that slice of
     the anchor-ordered pair list (bounded CPU baselines).  ``anchor_end`` (one per window)
     keeps only the pairs whose left SNP lies before it (a rank's share of a split parse).
+    ``stat_fn`` replaces the statistics function (``hap_stats`` signature), e.g. pg_gpu's
+    own kernels through ``oracle.ref_kernels.hap_stats``.
     """
     edges = np.asarray(edges, dtype=np.float64)
     nb = len(edges) - 1
@@ -760,7 +762,7 @@ def bin_sums(data, positions, pop_rows, edges, genotypes=False, chunk=200_000,
            "n_pairs": len(ii)}
     coord = np.asarray(positions if coords is None else coords, dtype=np.float64)
     count_fn = geno_counts if genotypes else hap_counts
-    stat_fn = geno_stats if genotypes else hap_stats
+    stat_fn = stat_fn or (geno_stats if genotypes else hap_stats)
     for s in range(0, len(ii), chunk):
         ci, cj = ii[s:s + chunk], jj[s:s + chunk]
         d = np.abs(coord[cj] - coord[ci])

@@ -179,3 +179,20 @@ def test_all_pairs_genotype_oracle_matches_reference(golden_dir):
     np.testing.assert_allclose(O.diploid_r2_matrix(g["geno_missing"]), g["diploid_r2"], rtol=1e-12, atol=1e-15)
     np.testing.assert_allclose(O.zns_diploid(g["geno_missing"]), g["zns_diploid"], rtol=1e-12)
     np.testing.assert_allclose(O.omega_diploid(g["geno_missing"]), g["omega_diploid"], rtol=1e-12)
+
+
+@pytest.mark.parametrize("P", [1, 3, 4])
+def test_reference_kernel_driver_reproduces_golden(ref_hap, P):
+    """oracle.ref_kernels (pg_gpu's own estimator kernels, host-compiled in oracle/_ref,
+    driven by a restatement of its dispatch) gives the statistics the reference itself
+    produced (golden fixture made by running pg_gpu's Python), on the golden counts with
+    missing data.  Runs where oracle/_ref has been built."""
+    from oracle import ref_kernels
+    if not ref_kernels.available():
+        pytest.skip("oracle/_ref not built")
+    g = ref_hap
+    counts = [g[f"P{P}_counts{p}"] for p in range(P)]
+    nvalid = [None if (g[f"P{P}_nvalid{p}"] == -1).all() else g[f"P{P}_nvalid{p}"] for p in range(P)]
+    got = ref_kernels.hap_stats(counts, nvalid)
+    np.testing.assert_allclose(got, g[f"P{P}_stats"], rtol=1e-14, atol=1e-300)
+    np.testing.assert_allclose(got, O.hap_stats(counts, nvalid), rtol=1e-12, atol=1e-15)
