@@ -634,7 +634,8 @@ __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
                             int hh, hv, vh, vv;
                             if (role == 0) { hh = (int)w[0]; hv = (int)w[1]; vh = (int)rx; vv = (int)ry; }
                             else { vh = (int)w[2]; vv = (int)w[3]; hh = (int)rx; hv = (int)ry; }
-                            hap_set_counts(f[p], T(hh), T(hv - hh), T(vh - hh), T(vv - hv - vh + hh));
+                            hap_set_counts(f[p], count_to<T>(hh), count_to<T>(hv - hh), count_to<T>(vh - hh),
+                                           count_to<T>(vv - hv - vh + hh));
                             nval[p] = vv;
                         }
                         if (valid && cur >= 0 && cur < nb) {
@@ -675,13 +676,15 @@ __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
                                 const int n01 = (int)G[2][0] - n11 - n21, n02 = (int)G[2][1] - n12 - n22;
                                 const int nv = (int)G[2][2];
                                 const int n00 = nv - n01 - n02 - n10 - n11 - n12 - n20 - n21 - n22;
-                                const T cd[9] = {T(n00), T(n01), T(n02), T(n10), T(n11), T(n12), T(n20), T(n21), T(n22)};
+                                const T cd[9] = {count_to<T>(n00), count_to<T>(n01), count_to<T>(n02),
+                                                 count_to<T>(n10), count_to<T>(n11), count_to<T>(n12),
+                                                 count_to<T>(n20), count_to<T>(n21), count_to<T>(n22)};
                                 if (p == 0) {
 #pragma unroll
                                     for (int m = 0; m < 9; ++m) c0[m] = cd[m];
                                 }
                                 geno_set_counts(f[p], cd);
-                                f[p].n = T(nv);
+                                f[p].n = count_to<T>(nv);
                                 if constexpr (P <= 3) {
                                     geno_prepare_from(f[p], a.gtab + nv);  // n = ns = nv here
                                     geno_features<T, P, false>(f[p]);

@@ -123,3 +123,15 @@ def test_pack_codes_round_trip():
         np.testing.assert_array_equal(parse.unpack_codes(p, n_var), x)
         v = n_var - 1
         np.testing.assert_array_equal((p[:, v // 4] >> (2 * (v % 4))) & 3, x[:, v] + 1)
+
+
+def test_exact_int_to_double_identity():
+    """The tensor-core epilogue converts counts with the 2^52 "magic number" method
+    (ldk_common.cuh: i2d_exact): the bit pattern 0x43300000:(x ^ 2^31) is the double
+    2^52 + 2^31 + x, and one subtraction returns x exactly.  Checked in NumPy's IEEE float64
+    over the int32 range ends and random values."""
+    rng = np.random.default_rng(3)
+    x = np.concatenate([np.array([0, 1, -1, 2**31 - 1, -2**31], np.int64),
+                        rng.integers(-2**31, 2**31, 200_000)]).astype(np.int32)
+    bits = (np.uint64(0x43300000) << np.uint64(32)) | (x.view(np.uint32) ^ np.uint32(0x80000000)).astype(np.uint64)
+    np.testing.assert_array_equal(bits.view(np.float64) - 4503601774854144.0, x.astype(np.float64))
