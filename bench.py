@@ -229,6 +229,17 @@ def make_workload(cfg, scale, rank):
     return synth.make_config(cfg, scale=scale, seed=seed)
 
 
+def bench_workload(args, rank):
+    """The configuration's workload, its rows regrouped into ``--pops`` populations if asked."""
+    w = make_workload(args.config, args.scale, rank)
+    if args.pops:
+        import dataclasses
+        rows = np.concatenate([np.asarray(r) for r in w.pop_rows])
+        w = dataclasses.replace(w, pop_rows=[np.asarray(x) for x in np.array_split(rows, args.pops)],
+                                name=f"{w.name}, rows regrouped into {args.pops} populations")
+    return w
+
+
 def algorithmic_int_ops_per_pair(w):
     """Count-stage INT ops per pair (MAC = 2): haplotypes, four 0/1 dot products of
     length n per population (h.h, h.v, v.h, v.v), i.e. 8n; genotypes, the 3 x 3 Gram of
@@ -252,6 +263,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="default tile width, no tuning")
     ap.add_argument("--packed", action="store_true",
                     help="inputs stored two bits per entry (parse.pack_codes): a quarter of the bytes to copy")
+    ap.add_argument("--pops", type=int, default=0,
+                    help="regroup the workload's sampled rows into this many populations of equal size")
     ap.add_argument("--split", action="store_true",
                     help="strong scaling: one workload split into anchor ranges over the ranks")
     ap.add_argument("--all-pairs", action="store_true",
@@ -279,7 +292,7 @@ def main():
     from pg_gpu_b200 import _lib, parse, synth
 
     lib = _lib.load()
-    w = make_workload(args.config, args.scale, 0 if args.split else rank)
+    w = bench_workload(args, 0 if args.split else rank)
     n_pairs = synth.count_pairs(w)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -678,7 +691,7 @@ def run_reference(args, ws, rank):
     cover the workload, else the oracle's restatement -- all host cores, bounded samples."""
     if ws > 1 and rank != 0:
         return
-    w = make_workload(args.config, args.scale, 0)
+    w = bench_workload(args, 0)
     cores = cpu_cores()
     # each step a bounded sample (~4 s of every core), so that K + W steps end in a few minutes
     per_step = max(2.0, min(args.cpu_seconds, 200.0 / max(1, args.steps + args.warmup)) / 4.0)

@@ -129,7 +129,7 @@ typedef struct {
  *    may cover at most 2 (genotypes: 4) consecutive bootstrap blocks from its first SNP's
  *    block; otherwise the parse stops with LDK_ERR_DEVICE and status LDK_DEVERR_BLOCK_SPAN;
  *  - the per-bin sums of the row block's bootstrap blocks must fit in shared memory beside
- *    the pipeline, else LDK_ERR_UNSUPPORTED (four genotype populations with more than 20
+ *    the pipeline, else LDK_ERR_UNSUPPORTED (four genotype populations with more than 36
  *    bins, three with more than 47). */
 
 typedef struct {

@@ -80,7 +80,9 @@ struct Cfg {
     static constexpr int REGIONS = GENO ? 3 : 1;                       // MMAs per K step and population
     static constexpr int COLS = P * REGIONS * N;                       // TMEM columns per buffer
     static constexpr int NBUF = 2 * COLS <= kTmemCols ? 2 : 1;         // accumulator buffers
-    static constexpr int STAGES = GENO ? 3 : (P == 1) ? 2 : (P == 2) ? 3 : 4;
+    // four genotype populations: two stages, so that the per-bin staging of more bins fits
+    // beside them (their epilogue, not the loads, sets the pace)
+    static constexpr int STAGES = GENO ? (P == 4 ? 2 : 3) : (P == 1) ? 2 : (P == 2) ? 3 : 4;
     static constexpr int A_BOX = 128 * kKChunk;                        // one 128-row A box
     static constexpr int A_BYTES = REGIONS * A_BOX;
     static constexpr int B_BYTES = N * kKChunk;
@@ -476,7 +478,8 @@ __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
         // SSPL (four haplotype populations): the two warps of a lane quarter split the
         // statistics, not the partners -- both take every pair, warp part 0 accumulates
         // statistics [0, K) and counts pairs, part 1 statistics [K, NS) and r^2 -- so that
-        // each holds about half of the 105 accumulators.
+        // each holds about half of the 105 accumulators.  (The same split of the genotype
+        // path measured slower: both warps then compute all four populations' features.)
         constexpr bool SSPL = !GENO && P == 4;
         constexpr int K = HapFusedSplit<P>::value;
         constexpr int NA = SSPL ? ((K > NS - K + 1 ? K : NS - K + 1)) : NS + 1;  // accumulators per lane

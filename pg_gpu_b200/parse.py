@@ -9,7 +9,7 @@ finite r^2.  Two counting/estimator methods:
 * ``"tc"``    -- INT8 tcgen05 Gram-product counts + FP64 estimators and bin sums;
 * ``"auto"``  -- ``"tc"``, or ``"plain"`` for the shapes the tensor-core kernel cannot stage
   (its per-bin sums must fit in shared memory beside the pipeline -- four genotype
-  populations with more than 20 bins do not -- and each 64-SNP (genotypes: 128-SNP) row
+  populations with more than 36 bins do not -- and each 64-SNP (genotypes: 128-SNP) row
   block may span at most two (four) bootstrap blocks).  Both are GPU kernels.
 
 ``Pipeline`` runs a stream of same-shape parses from pinned host memory with the copies

@@ -81,15 +81,15 @@ def test_pipeline_rejects_mismatched_inputs():
 
 
 def test_auto_method_switches_to_plain_where_tc_cannot_stage():
-    """Four genotype populations with 30 bins exceed the tensor-core kernel's shared-memory
-    staging: "tc" refuses with LDK_ERR_UNSUPPORTED, "auto" runs the plain FP64 kernel and
-    matches it; on a shape the tensor-core kernel stages, "auto" keeps it."""
+    """Four genotype populations with 40 bins exceed the tensor-core kernel's shared-memory
+    staging (36 bins fit): "tc" refuses with LDK_ERR_UNSUPPORTED, "auto" runs the plain FP64
+    kernel and matches it; on a shape the tensor-core kernel stages, "auto" keeps it."""
     from pg_gpu_b200 import _lib
     w = synth.make_config(3, scale=0.01)
     n = w.data.shape[0]
     q = n // 4
     rows = [np.arange(k * q, (k + 1) * q) for k in range(4)]
-    edges = np.linspace(0, w.max_dist, 31)
+    edges = np.linspace(0, w.max_dist, 41)
     with pytest.raises(_lib.LdkError) as e:
         parse.Parser(w.data, w.positions, rows, edges, genotypes=True, method="tc", max_dist=w.max_dist).run()
     assert e.value.code == _lib.LDK_ERR_UNSUPPORTED
