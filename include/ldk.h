@@ -245,6 +245,19 @@ LDK_API int ldk_autotune_save(const char* path);
 LDK_API int ldk_autotune_count(int* tunings);
 LDK_API int ldk_autotune_clear(void);
 
+/* Whether two parses with this descriptor give the same output bits whatever order the GPU
+ * runs their row blocks in: 1, or 0 where the bin sums agree only to FP64 rounding; a
+ * negative status for an invalid descriptor.  Every kernel adds its per-row-block partial
+ * sums as fixed-point integers (an order-independent sum); the partials themselves are a
+ * fixed function of the input when each epilogue warp of the tensor-core kernel stages its
+ * sums in its own shared-memory copy, and the plain kernel always.  Shapes whose staging
+ * does not fit once per warp (four populations; three genotype populations with more than
+ * five bins, three haplotype populations with more than about twenty) share one copy
+ * updated with shared-memory atomics, whose order varies.  Depends on the tile width in
+ * use (after tuning, the tuned one).  Host-only; no counterpart in pg_gpu (its cp.add.at
+ * bin sums, moments_ld.py:335-339, are order-dependent). */
+LDK_API int ldk_parse_reproducible(const ldk_parse_t* d);
+
 /* Row blocks of the tensor-core methods (genotypes 0: haplotype path, 1: genotype path):
  * *rows SNPs per row block, counted from each window's first SNP, and *max_blocks, the
  * bootstrap blocks one row block may cover from its first SNP's block (more stops the

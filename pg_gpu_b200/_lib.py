@@ -86,6 +86,7 @@ EXPORTS = {
     "ldk_autotune_save": (ctypes.c_int, [ctypes.c_char_p]),
     "ldk_autotune_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
     "ldk_autotune_clear": (ctypes.c_int, []),
+    "ldk_parse_reproducible": (ctypes.c_int, [ctypes.POINTER(ParseDesc)]),
     "ldk_tc_row_blocks": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]),
     "ldk_profile": (ctypes.c_int, [ctypes.c_int]),
     "ldk_profile_last_kernel_ms": (ctypes.c_double, []),

@@ -591,6 +591,15 @@ int ldk_tile_width(const ldk_parse_t* d) {
     return tc_tile_width(sh, v < 0 ? 0 : v);
 }
 
+int ldk_parse_reproducible(const ldk_parse_t* d) {
+    if (int rc = validate(d)) return rc;
+    if (d->method == LDK_METHOD_PLAIN_FP64) return 1;
+    ParseShape sh;
+    shape_of(d, sh);
+    const int v = tuned_variant(d, sh);
+    return tc_private_staging(sh, v < 0 ? 0 : v) ? 1 : 0;
+}
+
 int ldk_tc_row_blocks(int genotypes, int32_t* rows, int32_t* max_blocks) {
     if (!rows || !max_blocks) { set_error("null output pointer"); return LDK_ERR_ARG; }
     ParseShape sh{};

@@ -75,6 +75,7 @@ int tc_planes(const ParseShape& sh);
 cudaError_t probe_peaks(double* int8_ops_per_s, double* fp64_fma_per_s, unsigned* status, cudaStream_t s);
 size_t tc_smem_bytes(const ParseShape& sh);
 bool tc_rtab_global(const ParseShape& sh);  // where the reciprocal table must live
+bool tc_private_staging(const ParseShape& sh, int variant);  // one staging copy per epilogue warp
 cudaError_t launch_fill_rtab(void* rtab, int max_n, cudaStream_t s);
 cudaError_t launch_fill_gtab(void* gtab, int max_n, cudaStream_t s);
 

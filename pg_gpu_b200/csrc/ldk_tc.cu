@@ -188,6 +188,22 @@ size_t tc_smem_bytes(const ParseShape& sh) {
     return sh.genotypes ? tc_smem_bytes_g<true>(sh) : tc_smem_bytes_g<false>(sh);
 }
 
+template <bool GENO, int V>
+bool private_staging_of(const ParseShape& sh) {
+    const int t = smem_table(sh);
+    switch (sh.P) {
+        case 1: return private_staging<1, GENO, V>(sh.n_bins, t);
+        case 2: return private_staging<2, GENO, V>(sh.n_bins, t);
+        case 3: return private_staging<3, GENO, V>(sh.n_bins, t);
+        default: return private_staging<4, GENO, V>(sh.n_bins, t);
+    }
+}
+
+bool tc_private_staging(const ParseShape& sh, int variant) {
+    if (sh.genotypes) return (variant == 1 && sh.P <= 2) ? private_staging_of<true, 1>(sh) : private_staging_of<true, 0>(sh);
+    return variant == 1 ? private_staging_of<false, 1>(sh) : private_staging_of<false, 0>(sh);
+}
+
 bool tc_rtab_global(const ParseShape& sh) {
     switch (sh.P) {
         case 1: return rtab_global_t<1>(sh);

@@ -228,6 +228,13 @@ class Parser:
         _lib.check(rc)
         return self.out
 
+    def reproducible(self) -> bool:
+        """Whether repeated runs give identical bits (``ldk_parse_reproducible``)."""
+        r = self.lib.ldk_parse_reproducible(ctypes.byref(self.desc))
+        if r < 0:
+            _lib.check(r)
+        return bool(r)
+
     def tile_width(self):
         """Partner SNPs per tile this parse uses now (tuned or default); 0 for "plain"."""
         w = self.lib.ldk_tile_width(ctypes.byref(self.desc))

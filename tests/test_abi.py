@@ -109,3 +109,29 @@ def test_autotune_table_file_round_trip(tmp_path):
         _lib.autotune_load(str(bad))
     with pytest.raises(_lib.LdkError):
         _lib.autotune_load(str(tmp_path / "missing.json"))
+
+
+def test_reproducibility_query_without_gpu():
+    """ldk_parse_reproducible (host-only): the plain kernel and the tensor-core shapes with a
+    staging copy per epilogue warp (configurations 1-5) are bit-reproducible; four
+    populations and three genotype populations with more than five bins share one staging
+    copy and are not."""
+    import ctypes
+    lib = _lib.load()
+
+    def desc(P, geno, nb, n_each, method=_lib.METHOD_TC):
+        d = _lib.ParseDesc()
+        d.n_pops, d.genotypes, d.n_bins, d.n_blocks, d.method, d.max_dist = P, geno, nb, 1, method, 1.0
+        for k in range(nb + 1):
+            d.edges[k] = float(k)
+        for k in range(5):
+            d.pop_offsets[k] = min(k, P) * n_each
+        return d
+
+    cases = {(1, 0, 4, 100): 1, (2, 0, 16, 120): 1, (3, 0, 16, 160): 1, (1, 1, 20, 500): 1, (1, 0, 32, 2000): 1,
+             (4, 0, 16, 150): 0, (3, 1, 6, 160): 0, (3, 1, 5, 160): 1}
+    for (P, g, nb, n), want in cases.items():
+        assert lib.ldk_parse_reproducible(ctypes.byref(desc(P, g, nb, n))) == want, (P, g, nb, n)
+    assert lib.ldk_parse_reproducible(ctypes.byref(desc(4, 1, 16, 125, _lib.METHOD_PLAIN))) == 1
+    bad = desc(5, 0, 4, 10)
+    assert lib.ldk_parse_reproducible(ctypes.byref(bad)) == _lib.LDK_ERR_ARG
