@@ -35,10 +35,16 @@ constexpr int kPrepV = 128, kPrepK = 128;
 //   haplotypes  h = [x == 1], v = [x in {0, 1}]
 //   genotypes   [x == 1], [x == 2], [x in {0, 1, 2}], 0
 // Padding (127) and invalid codes give 0 in every plane; invalid codes also raise
-// LDK_DEVERR_BAD_INPUT.  PACKED: X holds 2-bit fields (code + 1), SNP v in bits 2 (v % 4) of
-// byte v / 4 of its row; four neighbouring threads read the same byte and each unpacks its
-// own field, so the gather moves a quarter of the bytes.
-template <bool GENO, bool PACKED>
+// LDK_DEVERR_BAD_INPUT.
+//
+// Gather forms.  WIDE (int8 input whose base address and row stride are multiples of four,
+// and every packed input): a lane takes four consecutive SNPs and a warp four consecutive K
+// rows; each row's four codes come in one load (a 32-bit word, or one packed byte whose four
+// 2-bit fields hold code + 1, SNP v in bits 2 (v % 4) of byte v / 4), the 4 x 4 byte block is
+// transposed in registers with byte permutes, and each SNP's four K bytes go to the tile in
+// one 32-bit store (the SNP order rotated by lane / 8 so that the 32 lanes' stores fall in 32
+// banks).  Otherwise one byte per load and store, one SNP per lane.
+template <bool GENO, bool PACKED, bool WIDE>
 __global__ void __launch_bounds__(256) k_prep_planes(PrepArgs a) {
     constexpr int PL = GENO ? 4 : 2;
     constexpr int RS = kPrepK + 4;  // bytes per SNP row: 33 words, so both the gather's byte
@@ -64,22 +70,66 @@ __global__ void __launch_bounds__(256) k_prep_planes(PrepArgs a) {
     constexpr int kThreads = 256, kRowStep = kThreads / kPrepV;
     static_assert(kThreads % kPrepV == 0 && kPrepK % kRowStep == 0, "gather geometry");
     bool bad = false;
-    {
+    if constexpr (WIDE) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        static_assert(kPrepV == 4 * 32 && kPrepK % (4 * (kThreads / 32)) == 0, "wide gather geometry");
+        const int64_t v = v0 + 4 * lane;
+        const int64_t left = a.n_var - v;
+        const int nv = left >= 4 ? 4 : (left > 0 ? (int)left : 0);  // SNPs of this quad in the matrix
+        // bytes of the quad outside the matrix read as padding (127)
+        const uint32_t keep = nv >= 4 ? 0xFFFFFFFFu : ((1u << (8 * nv)) - 1u);
+        const int8_t* base = a.X + (PACKED ? (v >> 2) : v);
+        const int rot = lane >> 3;
+        for (int kk = 4 * warp; kk < kPrepK; kk += 4 * (kThreads / 32)) {
+            uint32_t w[4];
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                const int row = srow[kk + m];
+                uint32_t x = 0x7F7F7F7Fu;
+                if (row >= 0 && nv > 0) {
+                    if constexpr (PACKED) {
+                        const uint32_t b = (uint8_t)__ldg(base + (int64_t)row * a.ld);
+                        // field j = code + 1 -> byte j = code (two's complement), or 0xFF for missing
+                        x = 0u;
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) x |= (((b >> (2 * j)) & 3u) - 1u & 0xFFu) << (8 * j);
+                    } else {
+                        x = __ldg(reinterpret_cast<const uint32_t*>(base + (int64_t)row * a.ld));
+                    }
+                    x = (x & keep) | (0x7F7F7F7Fu & ~keep);
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        if (j < nv) {
+                            const int8_t c = (int8_t)(x >> (8 * j));
+                            bad |= (c < -1 || c > xmax);
+                        }
+                    }
+                }
+                w[m] = x;
+            }
+            // 4 x 4 byte transpose: t[j] holds SNP j's codes of rows kk .. kk + 3
+            const uint32_t x0 = __byte_perm(w[0], w[1], 0x5140), x1 = __byte_perm(w[0], w[1], 0x7362);
+            const uint32_t x2 = __byte_perm(w[2], w[3], 0x5140), x3 = __byte_perm(w[2], w[3], 0x7362);
+            const uint32_t t[4] = {__byte_perm(x0, x2, 0x5410), __byte_perm(x0, x2, 0x7632),
+                                   __byte_perm(x1, x3, 0x5410), __byte_perm(x1, x3, 0x7632)};
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) {
+                const int j = (jj + rot) & 3;
+                *reinterpret_cast<uint32_t*>(tile + (4 * lane + j) * RS + kk) = t[j];
+            }
+        }
+    } else {
         const int vv = threadIdx.x % kPrepV, kb = threadIdx.x / kPrepV;
         const int64_t v = v0 + vv;
         const bool vin = v < a.n_var;
-        const int8_t* col = a.X + (PACKED ? (v >> 2) : v);
-        const int shift = 2 * (int)(v & 3);
+        const int8_t* col = a.X + v;
         int8_t* trow = tile + vv * RS;
 #pragma unroll 16
         for (int kk = kb; kk < kPrepK; kk += kRowStep) {
             const int row = srow[kk];
             int8_t x = 127;
             if (row >= 0 && vin) {
-                if constexpr (PACKED)
-                    x = (int8_t)((((unsigned)(uint8_t)__ldg(col + (int64_t)row * a.ld)) >> shift & 3u) - 1u);
-                else
-                    x = __ldg(col + (int64_t)row * a.ld);
+                x = __ldg(col + (int64_t)row * a.ld);
                 bad |= (x < -1 || x > xmax);
             }
             trow[kk] = x;
@@ -256,12 +306,16 @@ cudaError_t launch_prep_planes(const ldk_parse_t* d, const Scratch& w, const Par
     a.status = w.status;
     dim3 grid((unsigned)((d->n_var + kPrepV - 1) / kPrepV), (unsigned)(sh.ktot / kPrepK));
     const bool packed = d->x_format == LDK_X_PACKED2;
+    // 32-bit loads need every row start 4-byte aligned
+    const bool wide = packed || (reinterpret_cast<uintptr_t>(d->X) % 4 == 0 && d->ld_x % 4 == 0);
     if (sh.genotypes) {
-        if (packed) k_prep_planes<true, true><<<grid, 256, 0, s>>>(a);
-        else k_prep_planes<true, false><<<grid, 256, 0, s>>>(a);
+        if (packed) k_prep_planes<true, true, true><<<grid, 256, 0, s>>>(a);
+        else if (wide) k_prep_planes<true, false, true><<<grid, 256, 0, s>>>(a);
+        else k_prep_planes<true, false, false><<<grid, 256, 0, s>>>(a);
     } else {
-        if (packed) k_prep_planes<false, true><<<grid, 256, 0, s>>>(a);
-        else k_prep_planes<false, false><<<grid, 256, 0, s>>>(a);
+        if (packed) k_prep_planes<false, true, true><<<grid, 256, 0, s>>>(a);
+        else if (wide) k_prep_planes<false, false, true><<<grid, 256, 0, s>>>(a);
+        else k_prep_planes<false, false, false><<<grid, 256, 0, s>>>(a);
     }
     return cudaGetLastError();
 }

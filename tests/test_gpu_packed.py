@@ -63,3 +63,37 @@ def test_packed_pipeline_matches_resident():
     for o in outs:
         np.testing.assert_array_equal(o[0].numpy(), ref["sums"])
         np.testing.assert_array_equal(o[1].numpy(), ref["pairs"])
+
+
+@pytest.mark.parametrize("cfg,scale", [(4, 0.004), (3, 0.02)])
+def test_plane_gather_forms_agree(cfg, scale):
+    """The plane preparation's gather forms give the same planes: one byte per load (row
+    stride not a multiple of four), four SNPs per 32-bit load (the same matrix in a buffer
+    whose row stride is padded to a multiple of four) and the packed form; checked through
+    the parse outputs, bit for bit, with an odd SNP count."""
+    from pg_gpu_b200 import _lib
+    import ctypes
+    w = synth.make_config(cfg, scale=scale)
+    kw = _kw(w)
+    n_var = w.n_var if w.n_var % 2 else w.n_var - 1
+    if n_var != w.n_var:  # keep the window offsets valid: drop the last SNP of the last window
+        data, pos = w.data[:, :n_var], w.positions[:n_var]
+        if w.window_offsets is not None:
+            kw["window_offsets"] = np.concatenate([w.window_offsets[:-1], [n_var]])
+        if w.snp_block is not None:
+            kw["snp_block"] = w.snp_block[:n_var]
+    else:
+        data, pos = w.data, w.positions
+    p = parse.Parser(data, pos, w.pop_rows, w.edges, **kw)
+    assert p.desc.ld_x % 4 != 0
+    byte = {k: v.copy() for k, v in p.run().numpy().items()}
+    ld = (n_var + 15) // 16 * 16
+    padded = torch.zeros((data.shape[0], ld), dtype=torch.int8, device="cuda")
+    padded[:, :n_var] = torch.as_tensor(data, device="cuda")
+    p.desc.X, p.desc.ld_x = _lib.ptr(padded), ld
+    wide = {k: v.copy() for k, v in p.run().numpy().items()}
+    packed = parse.Parser(parse.pack_codes(data), pos, w.pop_rows, w.edges, packed=True, **kw).run().numpy()
+    assert byte["pairs"].sum() > 0
+    for k in ("pairs", "r2_counts", "sums", "r2_sums"):
+        np.testing.assert_array_equal(wide[k], byte[k])
+        np.testing.assert_array_equal(packed[k], byte[k])
