@@ -97,11 +97,15 @@ struct Cfg {
     //    registers up with setmaxnreg (kRegCtrl each) and the epilogue warps 4..11 take
     //    them (kRegEpi each), so that every scheduler holds two full-register epilogue
     //    warps beside one control warp.
-    //  * otherwise (one or two haplotype populations, ≤ 160 registers): 10 warps, TMA and
-    //    MMA in warps 0 and 1, the epilogue in warps 2..9 (168 registers at most, since two
-    //    schedulers hold three warps).
+    //  * two haplotype populations (≤ 160 registers): 10 warps, TMA and MMA in warps 0 and 1,
+    //    the epilogue in warps 2..9 (168 registers at most, since two schedulers hold three
+    //    warps).
+    //  * one haplotype population (about 100 registers): 18 warps, TMA and MMA in warps 0 and
+    //    1, sixteen epilogue warps 2..17, four per lane quarter and scheduler, each taking a
+    //    quarter of every partner tile -- its per-pair work is short, so more warps hide the
+    //    latency of its dependency chains (113 registers at most).
     static constexpr bool SPLIT = GENO || P >= 3;
-    static constexpr int EPI = 8;
+    static constexpr int EPI = (!GENO && P == 1) ? 16 : 8;
     static constexpr int W0 = SPLIT ? 4 : 2;  // first epilogue warp
     static constexpr int THREADS = 32 * (W0 + EPI);
     static_assert(NBUF * COLS <= kTmemCols, "TMEM budget");
