@@ -48,12 +48,11 @@ constexpr int kKChunk = 128;            // K bytes per TMA box / swizzle row
 constexpr int kRing = 2;                // claimed row blocks in flight between the roles
 constexpr int kTmemCols = 512;
 constexpr uint64_t kTimeoutNs = 5000000000ull;  // 5 s per wait
-// Register split of the SPLIT layout (384 threads): the launch gives every thread
-// kRegLaunch registers; warpgroup 0 drops to kRegCtrl and the two epilogue warpgroups rise
-// to kRegEpi, which the freed registers cover exactly.  The host launches only a kernel
-// compiled to kRegLaunch registers.
-constexpr int kRegLaunch = 168, kRegCtrl = 24, kRegEpi = 240;
-static_assert(4 * kRegCtrl + 8 * kRegEpi == 12 * kRegLaunch, "register split must use the launch allocation");
+// Register split of the SPLIT layouts: the launch gives every thread Cfg::REG_LAUNCH
+// registers; warpgroup 0 drops to kRegCtrl and the epilogue warpgroups rise to Cfg::REG_EPI,
+// which the freed registers cover (Cfg asserts the sum).  The host launches only a kernel
+// compiled to Cfg::REG_LAUNCH registers.
+constexpr int kRegCtrl = 24;
 constexpr size_t kMinSmem = 116 * 1024;
 constexpr size_t kMaxSmem = 227 * 1024;
 
@@ -66,9 +65,11 @@ constexpr size_t kMaxSmem = 227 * 1024;
 // Partners per tile: tile variant 0 is the default, variant 1 the alternative the
 // autotuner also times (half the width on the haplotype path; on the genotype path 8 for
 // one population, 16 for two -- one TMEM buffer -- and the default for more).
+// Two haplotype populations: 48 (or 24), so that each of the three epilogue warps of a lane
+// quarter takes an equal share of the tile.
 constexpr int tile_nj(int P, bool GENO, int V) {
     return GENO ? (V == 0 ? (P == 1 ? 16 : 8) : (P == 1 ? 8 : P == 2 ? 16 : 8))
-                : ((P == 1 ? 128 : P == 2 ? 64 : 32) >> V);
+                : ((P == 1 ? 128 : P == 2 ? 48 : 32) >> V);
 }
 
 template <int P, bool GENO = false, int V = 0>
@@ -91,23 +92,28 @@ struct Cfg {
     static constexpr int SLOTS = GENO ? 4 : 2;                         // bootstrap blocks staged per row block
     // Warp layout.  Warp w may read only TMEM lane quarter w % 4, and each of the four
     // schedulers of an SM holds warps w, w + 4, ... with a quarter of the register file.
-    // Eight epilogue warps, two per lane quarter, each take half of every partner tile.
+    // The epilogue warps of a lane quarter each take an equal share of every partner tile.
     //  * SPLIT (genotypes; haplotypes with three or four populations -- estimators that
     //    want ~240 registers): 12 warps.  Warpgroup 0 (TMA, MMA, two idle warps) gives its
-    //    registers up with setmaxnreg (kRegCtrl each) and the epilogue warps 4..11 take
-    //    them (kRegEpi each), so that every scheduler holds two full-register epilogue
-    //    warps beside one control warp.
-    //  * two haplotype populations (≤ 160 registers): 10 warps, TMA and MMA in warps 0 and 1,
-    //    the epilogue in warps 2..9 (168 registers at most, since two schedulers hold three
-    //    warps).
+    //    registers up with setmaxnreg (kRegCtrl each) and the eight epilogue warps 4..11
+    //    take them (240 each), so that every scheduler holds two full-register epilogue
+    //    warps beside one control warp (launch: 168 per thread).
+    //  * two haplotype populations (~155 registers), also SPLIT: 16 warps, twelve epilogue
+    //    warps 4..15 at 160 registers, three per scheduler and lane quarter (launch: 128).
     //  * one haplotype population (about 100 registers): 18 warps, TMA and MMA in warps 0 and
     //    1, sixteen epilogue warps 2..17, four per lane quarter and scheduler, each taking a
     //    quarter of every partner tile -- its per-pair work is short, so more warps hide the
     //    latency of its dependency chains (113 registers at most).
-    static constexpr bool SPLIT = GENO || P >= 3;
-    static constexpr int EPI = (!GENO && P == 1) ? 16 : 8;
+    static constexpr bool SPLIT = GENO || P >= 2;
+    static constexpr int EPI = (!GENO && P == 1) ? 16 : (!GENO && P == 2) ? 12 : 8;
     static constexpr int W0 = SPLIT ? 4 : 2;  // first epilogue warp
     static constexpr int THREADS = 32 * (W0 + EPI);
+    static constexpr int REG_LAUNCH = (EPI == 12) ? 128 : 168;  // SPLIT layouts only
+    static constexpr int REG_EPI = (EPI == 12) ? 160 : 240;
+    static_assert(!SPLIT || 4 * kRegCtrl + EPI * REG_EPI <= (W0 + EPI) * REG_LAUNCH,
+                  "register split must fit the launch allocation");
+    static_assert(!SPLIT || THREADS * REG_LAUNCH <= 65536, "register file");
+    static_assert(EPI % 4 == 0 && (GENO ? NJ : NJ / 2) % (EPI / 4) == 0, "epilogue warps share tiles equally");
     static_assert(NBUF * COLS <= kTmemCols, "TMEM budget");
     static_assert(N % 16 == 0 && N <= 256, "MMA N");
 };
@@ -464,7 +470,7 @@ __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
         if (warp == 0) run_producer<C>(pipe, &tmA, &tmB, a, lane);
         else if (warp == 1) run_mma<C, P>(pipe, tmem, a, lane);
     } else {
-        if constexpr (C::SPLIT) setmaxnreg_inc<kRegEpi>();
+        if constexpr (C::SPLIT) setmaxnreg_inc<C::REG_EPI>();
         // ------------------------------------------------------------- epilogue
         const int e = warp - C::W0;
         const int L = (warp & 3) * 32 + lane;
@@ -868,12 +874,12 @@ cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t* o, co
         cudaFuncSetAttribute(k_parse_tc<P, T, PRIV, GENO, V, GT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     if constexpr (C::SPLIT) {
-        // the register split adds up only at kRegLaunch registers per thread; any other
+        // the register split adds up only at C::REG_LAUNCH registers per thread; any other
         // allocation would leave setmaxnreg.inc waiting, so such a build is not launched
         cudaFuncAttributes fa;
         e = cudaFuncGetAttributes(&fa, k_parse_tc<P, T, PRIV, GENO, V, GT>);
         if (e != cudaSuccess) return e;
-        if (fa.numRegs != kRegLaunch) return cudaErrorInvalidKernelImage;
+        if (fa.numRegs != C::REG_LAUNCH) return cudaErrorInvalidKernelImage;
     }
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
