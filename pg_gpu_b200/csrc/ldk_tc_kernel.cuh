@@ -65,10 +65,10 @@ constexpr size_t kMaxSmem = 227 * 1024;
 // Partners per tile: tile variant 0 is the default, variant 1 the alternative the
 // autotuner also times (half the width on the haplotype path; on the genotype path 8 for
 // one population, 16 for two -- one TMEM buffer -- and the default for more).
-// Two haplotype populations: 48 (or 24), so that each of the three epilogue warps of a lane
-// quarter takes an equal share of the tile.
+// Two haplotype populations and one genotype population: 48 (or 24) and 12 (or 24), so that
+// each of the three epilogue warps of a lane quarter takes an equal share of the tile.
 constexpr int tile_nj(int P, bool GENO, int V) {
-    return GENO ? (V == 0 ? (P == 1 ? 16 : 8) : (P == 1 ? 8 : P == 2 ? 16 : 8))
+    return GENO ? (V == 0 ? (P == 1 ? 12 : 8) : (P == 1 ? 24 : P == 2 ? 16 : 8))
                 : ((P == 1 ? 128 : P == 2 ? 48 : 32) >> V);
 }
 
@@ -98,14 +98,15 @@ struct Cfg {
     //    registers up with setmaxnreg (kRegCtrl each) and the eight epilogue warps 4..11
     //    take them (240 each), so that every scheduler holds two full-register epilogue
     //    warps beside one control warp (launch: 168 per thread).
-    //  * two haplotype populations (~155 registers), also SPLIT: 16 warps, twelve epilogue
-    //    warps 4..15 at 160 registers, three per scheduler and lane quarter (launch: 128).
+    //  * two haplotype populations (~155 registers) and one genotype population, also SPLIT:
+    //    16 warps, twelve epilogue warps 4..15 at 160 registers, three per scheduler and lane
+    //    quarter (launch: 128).
     //  * one haplotype population (about 100 registers): 18 warps, TMA and MMA in warps 0 and
     //    1, sixteen epilogue warps 2..17, four per lane quarter and scheduler, each taking a
     //    quarter of every partner tile -- its per-pair work is short, so more warps hide the
     //    latency of its dependency chains (113 registers at most).
     static constexpr bool SPLIT = GENO || P >= 2;
-    static constexpr int EPI = (!GENO && P == 1) ? 16 : (!GENO && P == 2) ? 12 : 8;
+    static constexpr int EPI = (!GENO && P == 1) ? 16 : ((!GENO && P == 2) || (GENO && P == 1)) ? 12 : 8;
     static constexpr int W0 = SPLIT ? 4 : 2;  // first epilogue warp
     static constexpr int THREADS = 32 * (W0 + EPI);
     static constexpr int REG_LAUNCH = (EPI == 12) ? 128 : 168;  // SPLIT layouts only

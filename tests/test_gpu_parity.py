@@ -413,7 +413,7 @@ def test_autotune_picks_a_candidate_and_keeps_results(genotypes):
             kernel_ms.append(lib.ldk_profile_last_kernel_ms())
             np.testing.assert_array_equal(got["pairs"], want["pairs"])
             assert rel_err(got["sums"], want["sums"], 1e-300) < 1e-11
-        assert p.tile_width() in ({16, 8} if genotypes else {48, 24})
+        assert p.tile_width() in ({12, 24} if genotypes else {48, 24})
         # a parse launched on the candidates' spent row-block counter would finish at once
         assert kernel_ms[0] > 0.3 * kernel_ms[1], kernel_ms
     finally:
