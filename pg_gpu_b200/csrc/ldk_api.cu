@@ -181,7 +181,8 @@ int validate(const ldk_parse_t* d) {
 const char* status_text(unsigned s) {
     if (s & LDK_DEVERR_TIMEOUT) return "device wait timed out";
     if (s & LDK_DEVERR_BLOCK_RANGE) return "snp_block outside [0, n_blocks)";
-    if (s & LDK_DEVERR_BLOCK_SPAN) return "a 64-SNP row block spans more than two bootstrap blocks";
+    if (s & LDK_DEVERR_BLOCK_SPAN)
+        return "a tensor-core row block spans more bootstrap blocks than it stages (64 SNPs: two; genotypes, 128 SNPs: four)";
     if (s & LDK_DEVERR_ACCUM) return "a bin sum outside the fixed-point accumulator's range (|x| >= 2^63 or not finite)";
     if (s & LDK_DEVERR_BAD_INPUT) return "unsorted positions or coordinates, or allele codes outside {-1, 0, 1} (haplotypes) or {-1, 0, 1, 2} (genotypes)";
     return "device error";

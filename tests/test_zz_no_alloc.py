@@ -59,6 +59,26 @@ def test_noalloc_matches_workspace_entry_point(method, cfg, scale):
         _check_same(got, want, TOL[method])
 
 
+def test_noalloc_rank_slab_matches_workspace_entry_point():
+    """One rank's slab of an anchor split (anchors plus right halo, ``anchor_end``): the
+    no-allocation entry point lists its row blocks on the device, which must stop at the
+    anchor end as the host-built list of ldk_parse does."""
+    from pg_gpu_b200 import shard
+    lib = _lib.load()
+    w = synth.make_config(5, scale=0.01)
+    seg = shard.split_anchors(w.positions, [0, w.n_var], w.max_dist, 3)[1]
+    sw = shard.slab_workload(w, seg)
+    p = parse.Parser(sw.data, sw.positions, sw.pop_rows, sw.edges, method="tc", max_dist=sw.max_dist,
+                     window_offsets=sw.window_offsets, anchor_end=sw.anchor_end)
+    want = p.run()
+    torch.cuda.synchronize()
+    for _ in range(2):
+        got, o = _outputs_like(p)
+        _lib.check(lib.ldk_parse_noalloc(ctypes.byref(p.desc), ctypes.byref(o), _lib.stream_handle()))
+        torch.cuda.synchronize()
+        _check_same(got, want, TOL["tc"])
+
+
 def test_noalloc_rejects_oversized_parse():
     lib = _lib.load()
     rng = np.random.default_rng(5)
