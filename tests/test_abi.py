@@ -99,8 +99,10 @@ def test_autotune_table_file_round_trip(tmp_path):
     saved = json.loads(out.read_text())
     assert saved["format"] == "ldk-autotune"
     key = lambda e: (e["pops"], e["genotypes"], e["k_bytes"], e["bins"], e["cutoff_decade"], e["window_log2"])  # noqa
-    got = {key(e): (e["tile_variant"], e["order"], e["tile_partners"]) for e in saved["entries"]}
-    assert got == {key(e): (e["tile_variant"], e["order"], e["tile_partners"]) for e in entries}
+    got = {key(e): (e["tile_variant"], e["order"]) for e in saved["entries"]}
+    assert got == {key(e): (e["tile_variant"], e["order"]) for e in entries}
+    # the width is written from the library's tile table, not copied from the input
+    assert all(e["tile_partners"] > 0 for e in saved["entries"])
     _lib.autotune_clear()
     assert _lib.autotune_count()[0] == 0
     bad = tmp_path / "bad.json"
