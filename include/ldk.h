@@ -225,8 +225,8 @@ LDK_API int ldk_ld_matrix(const int8_t* X, int64_t ld_x, int64_t n_var, const in
  * candidate.  A shape class is (population count, haplotype or genotype path, padded sample
  * bytes, bin count, decade of max_dist, log2 of the mean window size).  Later ldk_parse,
  * ldk_parse_setup (the order) and ldk_parse_enqueue (the width) calls of the class use the
- * kept choice, tuning enabled or not; classes never tuned use the defaults (widest tile,
- * largest windows first).  ldk_tile_width returns the width (SNPs per partner tile) a call
+ * kept choice, tuning enabled or not; classes never tuned use the defaults (the widest
+ * haplotype tile, 12 / 8 partners for one / two genotype populations; largest windows first).  ldk_tile_width returns the width (SNPs per partner tile) a call
  * with this descriptor would use now, 0 for the plain method, or a negative status.  No
  * counterpart in pg_gpu. */
 LDK_API int ldk_autotune(int enable);
