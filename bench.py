@@ -588,13 +588,15 @@ def main():
                            w.data.nbytes >> 20, (w.n_var * 2 * parser_ktot(w)) >> 20)},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "roofline": roofline,
-            # per step: k_jmax, k_prep_planes, k_parse_tc, k_fx_finish, 2 x k_block_combine, and on
+            # per step: k_jmax, k_prep_planes, k_split_items, k_parse_tc, k_fx_finish,
+            # 2 x k_block_combine, and on
             # the genotype path (1-3 populations) k_fill_gtab; plain: k_jmax, k_parse_plain,
             # k_fx_finish, 2 x combine (a workspace reciprocal table, k_fill_rtab, serves only
             # populations whose table does not fit in shared memory: none of configurations 1-5)
             "gpu_launches": int(args.steps * (5 if parser.method == "plain" else
-                                              6 + int(bool(w.genotypes) and len(w.pop_rows) <= 3))),
-            "launch": "CUDA graph replay (memsets, k_jmax, planes + parse kernel, k_fx_finish, 2 x k_block_combine"
+                                              7 + int(bool(w.genotypes) and len(w.pop_rows) <= 3))),
+            "launch": "CUDA graph replay (memsets, k_jmax, planes, work items + parse kernel, k_fx_finish, "
+                      "2 x k_block_combine"
                       + (", genotype reciprocal table" if w.genotypes and parser.method != "plain" else "") + ")"
                       if not args.no_graph else "ldk_parse per step",
             "clocks": clocks,

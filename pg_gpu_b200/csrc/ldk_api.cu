@@ -60,9 +60,9 @@ int check_arch() {
 }
 
 struct Layout {
-    size_t status_off = 0, jmax_off = 0, win_off = 0, items_off = 0, hv_off = 0, rtab_off = 0, gtab_off = 0,
-           fx_off = 0, fx_bytes = 0, total = 0;
-    int n_items = 0;
+    size_t status_off = 0, jmax_off = 0, win_off = 0, rb_off = 0, items_off = 0, hv_off = 0, rtab_off = 0,
+           gtab_off = 0, fx_off = 0, fx_bytes = 0, total = 0;
+    int n_row_blocks = 0;
 };
 
 bool shape_of(const ldk_parse_t* d, ParseShape& sh) {
@@ -112,15 +112,17 @@ Layout layout_of(const ldk_parse_t* d, const ParseShape& sh) {
     L.fx_bytes = (size_t)d->n_blocks * d->n_bins * (sh.n_stats + 1) * kFxLimbs * sizeof(unsigned long long);
     off = align_up(off + L.fx_bytes, 256);
     if (d->method != LDK_METHOD_PLAIN_FP64) {
-        int n_items = 0;
+        int n_rb = 0;
         const int rows = tc_rows_per_block(sh);
         for (int w = 0; w < window_count(d); ++w) {
             const int64_t m = anchor_bound(d, w) - window_bound(d, w);
-            n_items += (int)((m + rows - 1) / rows);
+            n_rb += (int)((m + rows - 1) / rows);
         }
-        L.n_items = n_items;
+        L.n_row_blocks = n_rb;
+        L.rb_off = off;
+        off = align_up(off + (size_t)n_rb * 2 * sizeof(int32_t), 256);
         L.items_off = off;
-        off = align_up(off + (size_t)n_items * 2 * sizeof(int32_t), 1024);
+        off = align_up(off + (size_t)tc_item_capacity(n_rb) * 4 * sizeof(int32_t), 1024);
         L.hv_off = off;
         off = align_up(off + (size_t)d->n_var * sh.planes * sh.ktot, 256);
         if (sh.rtab_global) {
@@ -231,10 +233,12 @@ int prepare(const ldk_parse_t* d, void* workspace, size_t workspace_bytes, Prepa
     P.w.status = reinterpret_cast<unsigned*>(ws + P.L.status_off);
     P.w.row_counter = reinterpret_cast<int*>(ws + P.L.status_off + 64);
     P.w.item_counter = reinterpret_cast<int*>(ws + P.L.status_off + 128);
+    P.w.n_items = reinterpret_cast<int*>(ws + P.L.status_off + 192);
     P.w.jmax = reinterpret_cast<int32_t*>(ws + P.L.jmax_off);
     P.w.win_off = reinterpret_cast<int64_t*>(ws + P.L.win_off);
     P.w.anc_end = P.w.win_off + window_count(d) + 1;
     P.w.fx = reinterpret_cast<unsigned long long*>(ws + P.L.fx_off);
+    P.w.row_blocks = reinterpret_cast<int32_t*>(ws + P.L.rb_off);
     P.w.items = reinterpret_cast<int32_t*>(ws + P.L.items_off);
     P.w.hv = ws + P.L.hv_off;
     P.w.rtab = P.sh.rtab_global ? static_cast<void*>(ws + P.L.rtab_off) : nullptr;
@@ -254,7 +258,8 @@ int check_outputs(const ldk_parse_out_t* out) {
 
 // The tensor-core row-block list (64 SNPs for haplotypes, 128 for genotypes, up to each
 // window's anchor end) in claim order: 0 = the largest windows' row blocks first, 1 = window
-// order.  The kernel's CTAs claim row blocks in list order.
+// order.  Each launch splits it into work items (launch_split_items), which the kernel's
+// CTAs claim in list order.
 int upload_items(const ldk_parse_t* d, const Prepared& P, cudaStream_t s, int claim_order) {
     int rc;
     const int rows = tc_rows_per_block(P.sh);
@@ -264,17 +269,17 @@ int upload_items(const ldk_parse_t* d, const Prepared& P, cudaStream_t s, int cl
         std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
             return (window_bound(d, x + 1) - window_bound(d, x)) > (window_bound(d, y + 1) - window_bound(d, y));
         });
-    std::vector<int32_t> items;
-    items.reserve((size_t)P.L.n_items * 2);
+    std::vector<int32_t> rb;
+    rb.reserve((size_t)P.L.n_row_blocks * 2);
     for (int wi : order) {
         const int64_t ae = anchor_bound(d, wi);
         for (int64_t r0 = window_bound(d, wi); r0 < ae; r0 += rows) {
-            items.push_back((int32_t)r0);
-            items.push_back((int32_t)std::min<int64_t>(r0 + rows, ae));
+            rb.push_back((int32_t)r0);
+            rb.push_back((int32_t)std::min<int64_t>(r0 + rows, ae));
         }
     }
-    if (!items.empty() &&
-        (rc = check_cuda(cudaMemcpyAsync(P.w.items, items.data(), items.size() * sizeof(int32_t),
+    if (!rb.empty() &&
+        (rc = check_cuda(cudaMemcpyAsync(P.w.row_blocks, rb.data(), rb.size() * sizeof(int32_t),
                                          cudaMemcpyHostToDevice, s), "upload row blocks")))
         return rc;
     return LDK_OK;
@@ -347,6 +352,23 @@ int n_orders(const ldk_parse_t* d) { return window_count(d) > 1 ? 2 : 1; }
 int autotune_tc(const ldk_parse_t* dd, const ldk_parse_out_t* out, const Prepared& P, cudaStream_t s);
 int read_status(const unsigned* status_dev, cudaStream_t s);
 
+// The work items for tile variant `variant` (from this run's pair ranges), then the parse
+// kernel, its launch bracketed by the profiling events when `prof`.
+cudaError_t launch_tc(const ldk_parse_t* dd, const ldk_parse_out_t* out, const Prepared& P, int variant,
+                      cudaStream_t s, bool prof = false) {
+    const int n_rb = P.L.n_row_blocks;
+    if (n_rb == 0) {
+        if (prof) { cudaEventRecord(g_ev[0], s); cudaEventRecord(g_ev[1], s); }
+        return cudaSuccess;
+    }
+    cudaError_t e = launch_split_items(P.w, n_rb, tc_tile_width(P.sh, variant), s);
+    if (e != cudaSuccess) return e;
+    if (prof) cudaEventRecord(g_ev[0], s);
+    e = launch_parse_tc(dd, out, P.w, P.sh, tc_item_capacity(n_rb), variant, s);
+    if (prof) cudaEventRecord(g_ev[1], s);
+    return e;
+}
+
 int enqueue_device(const ldk_parse_t* d, const ldk_parse_out_t* out, const Prepared& P, cudaStream_t s, bool prof,
                    bool tune = false) {
     int rc;
@@ -368,10 +390,7 @@ int enqueue_device(const ldk_parse_t* d, const ldk_parse_out_t* out, const Prepa
             if ((rc = clear(&dd, out, P, s))) return rc;
         }
         const int v = tuned_variant(d, P.sh);
-        if (prof) cudaEventRecord(g_ev[0], s);
-        if ((rc = check_cuda(launch_parse_tc(&dd, out, P.w, P.sh, P.L.n_items, v < 0 ? 0 : v, s), "tensor-core parse")))
-            return rc;
-        if (prof) cudaEventRecord(g_ev[1], s);
+        if ((rc = check_cuda(launch_tc(&dd, out, P, v < 0 ? 0 : v, s, prof), "tensor-core parse"))) return rc;
         if ((rc = check_cuda(launch_fx_finish(&dd, out, P.w, P.sh.n_stats, s), "bin sums"))) return rc;
     }
     return LDK_OK;
@@ -395,7 +414,7 @@ int autotune_tc(const ldk_parse_t* dd, const ldk_parse_out_t* out, const Prepare
             for (int rep = 0; rep < 2 && fits && !rc; ++rep) {
                 if ((rc = clear(dd, out, P, s))) break;
                 cudaEventRecord(e0, s);
-                if (launch_parse_tc(dd, out, P.w, P.sh, P.L.n_items, v, s) != cudaSuccess) {
+                if (launch_tc(dd, out, P, v, s) != cudaSuccess) {
                     cudaGetLastError();  // this variant does not fit the shape (e.g. shared memory): skip it
                     fits = false;
                     break;

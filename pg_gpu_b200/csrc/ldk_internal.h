@@ -17,7 +17,10 @@ struct Scratch {
     int64_t* win_off;      // (n_windows + 1) window SNP offsets
     int64_t* anc_end;      // (n_windows) end of each window's anchor SNPs
     uint8_t* hv;           // TC path: (n_var, planes, Ktot) indicator planes
-    int32_t* items;        // TC path: (n_items, 2) row blocks
+    int32_t* row_blocks;   // TC path: (n_row_blocks, 2) row blocks [row0, row1) in claim order
+    int32_t* items;        // TC path: work items (row0, row1, t0, t1): rows [row0, row1),
+                           // partner tiles [t0, t1) of that row block
+    int* n_items;          // TC path: items in use
     void* rtab;            // TC haplotype path: (max_n + 1) double4 reciprocal table in the
                            // workspace, or null when it lives in shared memory
     void* gtab;            // TC genotype path: (max_n + 1) GenoRecip reciprocal table
@@ -80,6 +83,14 @@ cudaError_t launch_fill_rtab(void* rtab, int max_n, cudaStream_t s);
 cudaError_t launch_fill_gtab(void* gtab, int max_n, cudaStream_t s);
 
 cudaError_t launch_build_items(const Scratch& w, int n_windows, int rows, cudaStream_t s);
+// Work items of the tensor-core parse: each row block of w.row_blocks split into pieces of
+// at most c partner tiles of width nj, c = max(kMinItemTiles, ceil(total tiles / kItemTarget)),
+// from the pair ranges in w.jmax; the count goes to *w.n_items.  At most
+// n_row_blocks + kItemTarget items.
+constexpr int kItemTarget = 2048;
+constexpr int kMinItemTiles = 2;
+inline int tc_item_capacity(int n_row_blocks) { return n_row_blocks + kItemTarget; }
+cudaError_t launch_split_items(const Scratch& w, int n_row_blocks, int nj, cudaStream_t s);
 
 // all-pairs LD of one SNP set (ldk_ldm.cu)
 size_t ld_matrix_workspace(int64_t n_var, int32_t n_sel);

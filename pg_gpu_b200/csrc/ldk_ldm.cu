@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(128 + 32 * kLdmEpi, 1)
 
     __shared__ __align__(8) uint64_t full_bar[C::STAGES], empty_bar[C::STAGES], tfull[C::NBUF], tempty[C::NBUF];
     __shared__ __align__(8) uint64_t ifull[kRing], iempty[kRing];
-    __shared__ volatile int ring[kRing];
+    __shared__ volatile int ring[2 * kRing];
     __shared__ uint32_t tmem_base_s;
     __shared__ volatile int abort_s;
 
@@ -122,17 +122,17 @@ __global__ void __launch_bounds__(128 + 32 * kLdmEpi, 1)
             }
             item = __shfl_sync(0xffffffffu, item, 0);
             if (epi_bar_or<kLdmEpi>(abort_s != 0 || item < 0)) break;
-            const int row0 = a.items[2 * item], row1 = a.items[2 * item + 1];
-            const int jend = a.jmax[row1 - 1];
-            const int n_jt = jend > row0 + 1 ? (jend - row0 + NJ - 1) / NJ : 0;
+            int row0, row1, jt0;
+            const int n_jt = item_tiles<C>(a, item, row0, row1, jt0);
             if (n_jt == 0) continue;
+            const int jend = a.jmax[row1 - 1];
             const int i = row0 + quarter * 16 + rr;
             const bool row_ok = i < row1;
             const double pi = (EST == 0 && row_ok) ? m.psite[i] : 0.0;
             bool ok = true;
             for (int t = 0; t < n_jt; ++t, ++tcount) {
                 const uint32_t buf = tcount % C::NBUF, tph = (tcount / C::NBUF) & 1u;
-                const int j0 = row0 + t * NJ;
+                const int j0 = jt0 + t * NJ;
                 double preg[(kLdmHalf + 31) / 32];
 #pragma unroll
                 for (int kk = 0; kk < (kLdmHalf + 31) / 32; ++kk) {
@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(128 + 32 * kLdmGEpi, 1)
 
     __shared__ __align__(8) uint64_t full_bar[C::STAGES], empty_bar[C::STAGES], tfull[C::NBUF], tempty[C::NBUF];
     __shared__ __align__(8) uint64_t ifull[kRing], iempty[kRing];
-    __shared__ volatile int ring[kRing];
+    __shared__ volatile int ring[2 * kRing];
     __shared__ uint32_t tmem_base_s;
     __shared__ volatile int abort_s;
 
@@ -346,17 +346,17 @@ __global__ void __launch_bounds__(128 + 32 * kLdmGEpi, 1)
             }
             item = __shfl_sync(0xffffffffu, item, 0);
             if (epi_bar_or<kLdmGEpi>(abort_s != 0 || item < 0)) break;
-            const int row0 = a.items[2 * item], row1 = a.items[2 * item + 1];
-            const int jend = a.jmax[row1 - 1];
-            const int n_jt = jend > row0 + 1 ? (jend - row0 + NJ - 1) / NJ : 0;
+            int row0, row1, jt0;
+            const int n_jt = item_tiles<C>(a, item, row0, row1, jt0);
             if (n_jt == 0) continue;
+            const int jend = a.jmax[row1 - 1];
             const int i = row0 + quarter * 32 + lane;
             const bool row_ok = i < row1;
             const double mui = row_ok ? m.mu[i] : 0.0, vari = row_ok ? m.var[i] : 0.0;
             bool ok = true;
             for (int t = 0; t < n_jt; ++t, ++tcount) {
                 const uint32_t buf = tcount % C::NBUF, tph = (tcount / C::NBUF) & 1u;
-                const int j0 = row0 + t * NJ;
+                const int j0 = jt0 + t * NJ;
                 if (!mbar_wait(&tfull[buf], tph, &abort_s, a.status)) { ok = false; break; }
                 tc_fence_after();
 #pragma unroll 1
@@ -474,8 +474,8 @@ LdmLayout ldm_layout(int64_t n_var, int32_t n_sel, bool geno) {
     size_t off = 256;
     L.jmax = off;
     off = up(off + (size_t)n_var * 4, 256);
-    L.items = off;
-    off = up(off + (size_t)L.n_items * 8, 1024);
+    L.items = off;  // (row0, row1, 0, INT32_MAX): whole row blocks
+    off = up(off + (size_t)L.n_items * 16, 1024);
     L.planes = off;
     off = up(off + (size_t)n_var * (geno ? 4 : 2) * L.ktot, 256);
     L.psite = off;
@@ -547,12 +547,17 @@ cudaError_t launch_ld_matrix(const int8_t* X, int64_t ld_x, int64_t n_var, const
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const int rows_per_block = geno ? LdmGCfg::ROWS : LdmCfg::ROWS;
     std::vector<int32_t> it;
-    it.reserve((size_t)L.n_items * 2);
+    it.reserve((size_t)L.n_items * 4);
     for (int64_t r0 = 0; r0 < n_var; r0 += rows_per_block) {  // most partners first
         it.push_back((int32_t)r0);
         it.push_back((int32_t)std::min<int64_t>(r0 + rows_per_block, n_var));
+        it.push_back(0);
+        it.push_back(INT32_MAX);
     }
-    if ((e = cudaMemcpyAsync(items, it.data(), it.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s)) != cudaSuccess)
+    int* n_items = reinterpret_cast<int*>(ws + 192);
+    const int n_items_h = L.n_items;
+    if ((e = cudaMemcpyAsync(items, it.data(), it.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(n_items, &n_items_h, sizeof(int), cudaMemcpyHostToDevice, s)) != cudaSuccess)
         return e;
     if (estimator == LDK_LDM_R2) {
         k_site_freq<<<(unsigned)((n_var + 255) / 256), 256, 0, s>>>(X, ld_x, n_var, rows, n_sel, psite);
@@ -593,7 +598,7 @@ cudaError_t launch_ld_matrix(const int8_t* X, int64_t ld_x, int64_t n_var, const
     TcArgs a{};
     a.jmax = jmax;
     a.items = items;
-    a.n_items = L.n_items;
+    a.n_items = n_items;
     a.item_counter = reinterpret_cast<int*>(ws + 128);
     a.nkc = L.ktot / kKChunk;
     for (int p = 0; p <= LDK_MAX_POPS; ++p) a.kofs[p] = sh.kofs[p];

@@ -412,14 +412,14 @@ cudaError_t launch_parse_plain_t(const PlainArgs& a, int nb, cudaStream_t s) {
 // Row blocks of 64 (genotypes: 128) anchor SNPs per window, in window order (one thread: a
 // setup step).
 __global__ void k_build_items(const int64_t* __restrict__ win_off, const int64_t* __restrict__ anc_end, int n_win,
-                              int rows, int32_t* __restrict__ items) {
+                              int rows, int32_t* __restrict__ row_blocks) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     int k = 0;
     for (int wi = 0; wi < n_win; ++wi)
         for (int64_t r0 = win_off[wi]; r0 < anc_end[wi]; r0 += rows) {
-            items[2 * k] = (int32_t)r0;
+            row_blocks[2 * k] = (int32_t)r0;
             const int64_t r1 = r0 + rows < anc_end[wi] ? r0 + rows : anc_end[wi];
-            items[2 * k + 1] = (int32_t)r1;
+            row_blocks[2 * k + 1] = (int32_t)r1;
             ++k;
         }
 }
@@ -541,7 +541,7 @@ cudaError_t launch_parse_plain(const ldk_parse_t* d, const ldk_parse_out_t* o, c
 }
 
 cudaError_t launch_build_items(const Scratch& w, int n_windows, int rows, cudaStream_t s) {
-    k_build_items<<<1, 1, 0, s>>>(w.win_off, w.anc_end, n_windows, rows, w.items);
+    k_build_items<<<1, 1, 0, s>>>(w.win_off, w.anc_end, n_windows, rows, w.row_blocks);
     return cudaGetLastError();
 }
 

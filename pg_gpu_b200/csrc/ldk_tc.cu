@@ -320,6 +320,87 @@ cudaError_t launch_prep_planes(const ldk_parse_t* d, const Scratch& w, const Par
     return cudaGetLastError();
 }
 
+namespace {
+// Work items of the persistent parse kernel.  A row block alone is too coarse a unit where
+// there are few row blocks per SM (a 5,000-SNP window has 79) or where their count leaves a
+// partial last wave; pieces of at most c partner tiles bound the spread of the CTAs' finishing
+// times by one piece.  c = max(kMinItemTiles, ceil(total tiles / kItemTarget)), so shapes with
+// many small row blocks keep one item per row block.  Pieces of one row block are consecutive
+// (the claim order of the row blocks stays), its last piece runs to INT32_MAX, and a row block
+// without partners gets no item.  One block of 1024 threads: the total, then a block-wide
+// scan of the pieces per row block, 1024 row blocks per round.
+constexpr int kSplitThreads = 1024;
+
+__device__ __forceinline__ int rb_tiles(const int32_t* __restrict__ rb, const int32_t* __restrict__ jmax, int k,
+                                        int nj) {
+    const int r0 = rb[2 * k], r1 = rb[2 * k + 1];
+    const int jend = jmax[r1 - 1];
+    return jend > r0 + 1 ? (jend - r0 + nj - 1) / nj : 0;
+}
+
+__global__ void __launch_bounds__(kSplitThreads) k_split_items(const int32_t* __restrict__ rb, int n_rb,
+                                                               const int32_t* __restrict__ jmax, int nj,
+                                                               int4* __restrict__ items, int* __restrict__ n_items) {
+    __shared__ long long s_sum[kSplitThreads / 32];
+    __shared__ int s_scan[kSplitThreads / 32];
+    __shared__ int s_base;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    constexpr int NW = kSplitThreads / 32;
+    long long t = 0;
+    for (int k = tid; k < n_rb; k += kSplitThreads) t += rb_tiles(rb, jmax, k, nj);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) s_sum[wid] = t;
+    if (tid == 0) s_base = 0;
+    __syncthreads();
+    long long total = 0;
+#pragma unroll 4
+    for (int x = 0; x < NW; ++x) total += s_sum[x];
+    const long long cl = (total + kItemTarget - 1) / kItemTarget;
+    const int c = cl > kMinItemTiles ? (int)cl : kMinItemTiles;
+    for (int b0 = 0; b0 < n_rb; b0 += kSplitThreads) {
+        const int k = b0 + tid;
+        const int nt = k < n_rb ? rb_tiles(rb, jmax, k, nj) : 0;
+        const int parts = (nt + c - 1) / c;
+        int x = parts;  // inclusive scan within the warp, then over the warps
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) s_scan[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            int v = s_scan[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, v, o);
+                if (lane >= o) v += y;
+            }
+            s_scan[lane] = v;
+        }
+        __syncthreads();
+        const int first = s_base + (wid ? s_scan[wid - 1] : 0) + x - parts;
+        if (parts) {
+            const int r0 = rb[2 * k], r1 = rb[2 * k + 1];
+            for (int q = 0; q < parts; ++q)
+                items[first + q] = make_int4(r0, r1, q * c, q == parts - 1 ? INT32_MAX : (q + 1) * c);
+        }
+        const int round_total = s_scan[NW - 1];
+        __syncthreads();
+        if (tid == 0) s_base += round_total;
+        __syncthreads();
+    }
+    if (tid == 0) *n_items = s_base;
+}
+}  // namespace
+
+cudaError_t launch_split_items(const Scratch& w, int n_row_blocks, int nj, cudaStream_t s) {
+    k_split_items<<<1, kSplitThreads, 0, s>>>(w.row_blocks, n_row_blocks, w.jmax, nj,
+                                              reinterpret_cast<int4*>(w.items), w.n_items);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_parse_tc(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w,
                             const ParseShape& sh, int n_items, int variant, cudaStream_t s) {
     if (sh.genotypes) return launch_tc_geno(d, o, w, sh, n_items, variant, s);

@@ -45,7 +45,7 @@ namespace ldk {
 namespace {
 
 constexpr int kKChunk = 128;            // K bytes per TMA box / swizzle row
-constexpr int kRing = 2;                // claimed row blocks in flight between the roles
+constexpr int kRing = 2;                // claimed work items in flight between the roles
 constexpr int kTmemCols = 512;
 constexpr uint64_t kTimeoutNs = 5000000000ull;  // 5 s per wait
 // Register split of the SPLIT layouts: the launch gives every thread Cfg::REG_LAUNCH
@@ -261,9 +261,9 @@ struct TcArgs {
     const int32_t* jmax;
     const int32_t* snp_block;
     int n_blocks;
-    const int32_t* items;  // (n_items, 2): [row0, row1) row blocks
-    int n_items;
-    int* item_counter;     // next unclaimed row block (zero at launch)
+    const int32_t* items;  // (n_items, 4): rows [row0, row1), partner tiles [t0, t1) of that row block
+    const int* n_items;    // items in use (written with the list)
+    int* item_counter;     // next unclaimed item (zero at launch)
     int nkc;               // K chunks of 128 bytes
     int kofs[LDK_MAX_POPS + 1];
     int max_n;             // largest population (reciprocal table size - 1)
@@ -286,17 +286,25 @@ struct Pipe {
     uint64_t* tempty;
     uint64_t* ifull;
     uint64_t* iempty;
-    volatile int* ring;
+    volatile int* ring;  // [kRing] claimed items, then [kRing] their tile counts
     volatile int* abort_s;
 };
 
-// Partner tiles of row block `item` (rows [row0, row1), partners up to jmax[row1 - 1]).
+// Item `item`: rows [row0, row1) and the partner tiles [t0, t1) of that row block, t1
+// clipped to the row block's tiles (partners up to jmax[row1 - 1]).  Returns the number of
+// tiles; the first starts at partner jt0.  The items of one row block partition its tile
+// indices (its last item runs to INT32_MAX), so every tile is counted once whatever the
+// partner range is when the kernel runs.
 template <class C>
-LDK_DEV int tile_count(const TcArgs& a, int item, int& row0) {
-    row0 = a.items[2 * item];
-    const int row1 = a.items[2 * item + 1];
+LDK_DEV int item_tiles(const TcArgs& a, int item, int& row0, int& row1, int& jt0) {
+    const int4 it = reinterpret_cast<const int4*>(a.items)[item];
+    row0 = it.x;
+    row1 = it.y;
     const int jend = a.jmax[row1 - 1];
-    return jend > row0 + 1 ? (jend - row0 + C::NJ - 1) / C::NJ : 0;
+    const int n_jt = jend > row0 + 1 ? (jend - row0 + C::NJ - 1) / C::NJ : 0;
+    const int te = it.w < n_jt ? it.w : n_jt;
+    jt0 = row0 + it.z * C::NJ;
+    return te > it.z ? te - it.z : 0;
 }
 
 // TMA loads of K chunk c of the tile (row block at row0, partners from j0) into stage s.
@@ -332,8 +340,8 @@ LDK_DEV void issue_mmas(const Pipe& S, uint32_t tmem, const TcArgs& a, int s, in
     mma_commit(&S.empty_bar[s]);
 }
 
-// Warp 0: claims row blocks from the global counter, publishes them through the ring and
-// issues the TMA loads of every partner tile's K chunks.
+// Warp 0: claims work items from the global counter, publishes each with its tile count
+// through the ring and issues the TMA loads of every partner tile's K chunks.
 template <class C>
 LDK_DEV void run_producer(const Pipe& S, const CUtensorMap* tmA, const CUtensorMap* tmB, const TcArgs& a,
                           int lane) {
@@ -341,22 +349,24 @@ LDK_DEV void run_producer(const Pipe& S, const CUtensorMap* tmA, const CUtensorM
         uint32_t it = 0;
         bool ok = true;
         for (uint32_t k = 0; ok; ++k) {
-            // claim the next row block and publish it to the MMA issuer and the epilogue
+            // claim the next item and publish it to the MMA issuer and the epilogue
             const int sl = k % kRing;
             if (!mbar_wait(&S.iempty[sl], ((k / kRing) & 1u) ^ 1u, S.abort_s, a.status)) { ok = false; break; }
             int item = atomicAdd(a.item_counter, 1);
-            if (item >= a.n_items) item = -1;
+            if (item >= *a.n_items) item = -1;
+            int row0 = 0, row1 = 0, jt0 = 0, n_jt = 0;
+            if (item >= 0) n_jt = item_tiles<C>(a, item, row0, row1, jt0);
             S.ring[sl] = item;
+            S.ring[kRing + sl] = n_jt;
             mbar_arrive(&S.ifull[sl]);
             if (item < 0) break;
-            int row0;
-            const int n_jt = tile_count<C>(a, item, row0);
-            for (int t = 0; t < n_jt && ok; ++t) {
+            const int jstop = jt0 + n_jt * C::NJ;
+            for (int j0 = jt0; j0 < jstop && ok; j0 += C::NJ) {
                 for (int c = 0; c < a.nkc; ++c, ++it) {
                     const int s = it % C::STAGES;
                     const uint32_t ph = (it / C::STAGES) & 1u;
                     if (!mbar_wait(&S.empty_bar[s], ph ^ 1u, S.abort_s, a.status)) { ok = false; break; }
-                    issue_loads<C>(S, tmA, tmB, s, c, row0, row0 + t * C::NJ);
+                    issue_loads<C>(S, tmA, tmB, s, c, row0, j0);
                 }
             }
         }
@@ -374,11 +384,9 @@ LDK_DEV void run_mma(const Pipe& S, uint32_t tmem, const TcArgs& a, int lane) {
         for (uint32_t k = 0; ok; ++k) {
             const int sl = k % kRing;
             if (!mbar_wait(&S.ifull[sl], (k / kRing) & 1u, S.abort_s, a.status)) { ok = false; break; }
-            const int item = S.ring[sl];
+            const int item = S.ring[sl], n_jt = S.ring[kRing + sl];
             mbar_arrive(&S.iempty[sl]);
             if (item < 0) break;
-            int row0;
-            const int n_jt = tile_count<C>(a, item, row0);
             for (int t = 0; t < n_jt && ok; ++t, ++tcount) {
                 const uint32_t buf = tcount % C::NBUF, tph = (tcount / C::NBUF) & 1u;
                 if (!mbar_wait(&S.tempty[buf], tph ^ 1u, S.abort_s, a.status)) { ok = false; break; }
@@ -420,7 +428,7 @@ __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
 
     __shared__ __align__(8) uint64_t full_bar[C::STAGES], empty_bar[C::STAGES], tfull[C::NBUF], tempty[C::NBUF];
     __shared__ __align__(8) uint64_t ifull[kRing], iempty[kRing];
-    __shared__ volatile int ring[kRing];
+    __shared__ volatile int ring[2 * kRing];
     __shared__ uint32_t tmem_base_s;
     __shared__ volatile int abort_s;
     __shared__ double sedges[LDK_MAX_BINS + 1];
@@ -509,10 +517,15 @@ __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
             }
             item = __shfl_sync(0xffffffffu, item, 0);
             if (epi_bar_or<EPI>(abort_s != 0 || item < 0)) break;
-            const int row0 = a.items[2 * item], row1 = a.items[2 * item + 1];
+            // the item's tiles [tb, te) of row block [row0, row1) (as item_tiles; scalar loads
+            // and a loop over tile indices keep this 240-register epilogue free of spills)
+            const int row0 = a.items[4 * item], row1 = a.items[4 * item + 1];
             const int jend = a.jmax[row1 - 1];
-            const int n_jt = jend > row0 + 1 ? (jend - row0 + C::NJ - 1) / C::NJ : 0;
-            if (n_jt == 0) continue;
+            const int n_full = jend > row0 + 1 ? (jend - row0 + C::NJ - 1) / C::NJ : 0;
+            const int tw = a.items[4 * item + 3];
+            const int tb = a.items[4 * item + 2];
+            const int te = tw < n_full ? tw : n_full;
+            if (te <= tb) continue;
             const int i = row0 + r;
             bool row_ok = i < row1;
             const int my_jmax = row_ok ? a.jmax[i] : 0;
@@ -583,7 +596,7 @@ __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
                 }
             };
             bool ok = true;
-            for (int t = 0; t < n_jt; ++t, ++tcount) {
+            for (int t = tb; t < te; ++t, ++tcount) {
                 const uint32_t buf = tcount % C::NBUF, tph = (tcount / C::NBUF) & 1u;
                 const int j0 = row0 + t * C::NJ;
                 // partner coordinates of this tile, one per lane and register
@@ -853,7 +866,7 @@ cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t* o, co
     a.snp_block = d->snp_block;
     a.n_blocks = d->n_blocks;
     a.items = w.items;
-    a.n_items = n_items;
+    a.n_items = w.n_items;
     a.item_counter = w.item_counter;
     a.nkc = sh.ktot / kKChunk;
     for (int p = 0; p <= LDK_MAX_POPS; ++p) a.kofs[p] = sh.kofs[p];
