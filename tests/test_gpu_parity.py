@@ -392,6 +392,34 @@ def test_parse_graph_replay_matches_run(method):
     assert rel_err(got["sums"], want["sums"], 1e-300) > 1e-6  # the replay saw the new data
 
 
+@pytest.mark.parametrize("cfg,stretch", [(1, 3.0), (3, 20.0)])
+def test_graph_replay_after_positions_change(cfg, stretch):
+    """The tensor-core work items (runs of a row block's partner tiles) are split on the
+    device from each run's own pair ranges.  Captured once, then replayed after the SNP
+    positions are stretched in place (SNPs lose the partners that move beyond the cutoff,
+    so the split differs from the captured run's), a replay counts every pair once:
+    bit-equal to a fresh parse of the new positions and within the tolerance of the oracle
+    (haplotypes and genotypes)."""
+    w = synth.make_config(cfg, scale={1: 0.3, 3: 0.01}[cfg])
+    kw = dict(genotypes=w.genotypes, method="tc", max_dist=w.max_dist, window_offsets=w.window_offsets,
+              snp_block=w.snp_block, n_blocks=w.n_blocks)
+    p = parse.Parser(w.data, w.positions, w.pop_rows, w.edges, **kw)
+    before = {k: v.copy() for k, v in p.run().numpy().items()}
+    g, _ = p.graph()
+    pos2 = w.positions[0] + (w.positions - w.positions[0]) * stretch
+    p.pos.copy_(torch.as_tensor(pos2, device="cuda"))
+    g.replay()
+    p.status()
+    got = p.out.numpy()
+    fresh = parse.ld_parse(w.data, pos2, w.pop_rows, w.edges, **kw).numpy()
+    for k in ("pairs", "r2_counts", "sums", "r2_sums"):
+        np.testing.assert_array_equal(got[k], fresh[k])
+    want = O.bin_sums(w.data, pos2, w.pop_rows, w.edges, max_dist=w.max_dist, window_offsets=w.window_offsets,
+                      snp_block=w.snp_block, n_blocks=w.n_blocks, genotypes=bool(w.genotypes))
+    check_parse(got, want, TC_RTOL)
+    assert got["pairs"].sum() != before["pairs"].sum()
+
+
 @pytest.mark.parametrize("genotypes", [False, True])
 def test_autotune_picks_a_candidate_and_keeps_results(genotypes):
     """With tuning on, the first parse of a shape times the tile candidates and keeps one;
