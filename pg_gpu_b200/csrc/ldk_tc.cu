@@ -37,18 +37,21 @@ constexpr int kPrepV = 128, kPrepK = 128;
 // Padding (127) and invalid codes give 0 in every plane; invalid codes also raise
 // LDK_DEVERR_BAD_INPUT.
 //
-// Gather forms.  WIDE (int8 input whose base address and row stride are multiples of four,
-// and every packed input): a lane takes four consecutive SNPs and a warp four consecutive K
-// rows; each row's four codes come in one load (a 32-bit word, or one packed byte whose four
-// 2-bit fields hold code + 1, SNP v in bits 2 (v % 4) of byte v / 4), the 4 x 4 byte block is
+// Gather: a lane takes four consecutive SNPs and a warp four consecutive K rows; each row's
+// four codes come as one 32-bit word (int8 input) or one byte (packed input: four 2-bit
+// fields holding code + 1, SNP v in bits 2 (v % 4) of byte v / 4), the 4 x 4 byte block is
 // transposed in registers with byte permutes, and each SNP's four K bytes go to the tile in
 // one 32-bit store (the SNP order rotated by lane / 8 so that the 32 lanes' stores fall in 32
-// banks).  Otherwise one byte per load and store, one SNP per lane.
-template <bool GENO, bool PACKED, bool WIDE>
+// banks).  An int8 row segment that does not start on a 4-byte boundary (odd row stride, or
+// an unaligned base) is read as the two aligned words around it and joined with a funnel
+// shift; the offset is the same for the 32 lanes of a row, so the branch is warp-uniform.
+// The second word is read only where it holds SNPs of the quad, and an aligned word holding
+// one byte of the matrix lies in that byte's memory page, so no read can fault; its other
+// bytes are shifted or masked out.
+template <bool GENO, bool PACKED>
 __global__ void __launch_bounds__(256) k_prep_planes(PrepArgs a) {
     constexpr int PL = GENO ? 4 : 2;
-    constexpr int RS = kPrepK + 4;  // bytes per SNP row: 33 words, so both the gather's byte
-                                    // stores (one SNP per lane) and the scatter's word loads
+    constexpr int RS = kPrepK + 4;  // bytes per SNP row: 33 words, so the scatter's word loads
                                     // (one K quad per lane) hit distinct banks
     __shared__ __align__(16) int8_t tile[kPrepV * RS];
     __shared__ int srow[kPrepK];
@@ -64,13 +67,10 @@ __global__ void __launch_bounds__(256) k_prep_planes(PrepArgs a) {
         srow[kk] = (local >= 0 && local < np && k < a.kofs[a.P]) ? a.pop_rows[a.pop_off[p] + local] : -1;
     }
     __syncthreads();
-    // gather: tile[v][k] = X[row(k), v0 + v]; 127 marks padding.  Each thread keeps one SNP
-    // column (a warp reads 32 consecutive bytes of a row) and walks every second K row, 16
-    // loads in flight.
-    constexpr int kThreads = 256, kRowStep = kThreads / kPrepV;
-    static_assert(kThreads % kPrepV == 0 && kPrepK % kRowStep == 0, "gather geometry");
+    // gather: tile[v][k] = X[row(k), v0 + v]; 127 marks padding
+    constexpr int kThreads = 256;
     bool bad = false;
-    if constexpr (WIDE) {
+    {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         static_assert(kPrepV == 4 * 32 && kPrepK % (4 * (kThreads / 32)) == 0, "wide gather geometry");
         const int64_t v = v0 + 4 * lane;
@@ -94,7 +94,14 @@ __global__ void __launch_bounds__(256) k_prep_planes(PrepArgs a) {
 #pragma unroll
                         for (int j = 0; j < 4; ++j) x |= (((b >> (2 * j)) & 3u) - 1u & 0xFFu) << (8 * j);
                     } else {
-                        x = __ldg(reinterpret_cast<const uint32_t*>(base + (int64_t)row * a.ld));
+                        const uintptr_t ad = reinterpret_cast<uintptr_t>(base + (int64_t)row * a.ld);
+                        const uint32_t* q = reinterpret_cast<const uint32_t*>(ad & ~uintptr_t(3));
+                        const int s = (int)(ad & 3u);
+                        x = __ldg(q);
+                        if (s != 0) {
+                            const uint32_t hi = s + nv > 4 ? __ldg(q + 1) : 0u;
+                            x = __funnelshift_r(x, hi, 8 * s);
+                        }
                     }
                     x = (x & keep) | (0x7F7F7F7Fu & ~keep);
 #pragma unroll
@@ -117,22 +124,6 @@ __global__ void __launch_bounds__(256) k_prep_planes(PrepArgs a) {
                 const int j = (jj + rot) & 3;
                 *reinterpret_cast<uint32_t*>(tile + (4 * lane + j) * RS + kk) = t[j];
             }
-        }
-    } else {
-        const int vv = threadIdx.x % kPrepV, kb = threadIdx.x / kPrepV;
-        const int64_t v = v0 + vv;
-        const bool vin = v < a.n_var;
-        const int8_t* col = a.X + v;
-        int8_t* trow = tile + vv * RS;
-#pragma unroll 16
-        for (int kk = kb; kk < kPrepK; kk += kRowStep) {
-            const int row = srow[kk];
-            int8_t x = 127;
-            if (row >= 0 && vin) {
-                x = __ldg(col + (int64_t)row * a.ld);
-                bad |= (x < -1 || x > xmax);
-            }
-            trow[kk] = x;
         }
     }
     if (bad) atomicOr(a.status, LDK_DEVERR_BAD_INPUT);
@@ -306,16 +297,12 @@ cudaError_t launch_prep_planes(const ldk_parse_t* d, const Scratch& w, const Par
     a.status = w.status;
     dim3 grid((unsigned)((d->n_var + kPrepV - 1) / kPrepV), (unsigned)(sh.ktot / kPrepK));
     const bool packed = d->x_format == LDK_X_PACKED2;
-    // 32-bit loads need every row start 4-byte aligned
-    const bool wide = packed || (reinterpret_cast<uintptr_t>(d->X) % 4 == 0 && d->ld_x % 4 == 0);
     if (sh.genotypes) {
-        if (packed) k_prep_planes<true, true, true><<<grid, 256, 0, s>>>(a);
-        else if (wide) k_prep_planes<true, false, true><<<grid, 256, 0, s>>>(a);
-        else k_prep_planes<true, false, false><<<grid, 256, 0, s>>>(a);
+        if (packed) k_prep_planes<true, true><<<grid, 256, 0, s>>>(a);
+        else k_prep_planes<true, false><<<grid, 256, 0, s>>>(a);
     } else {
-        if (packed) k_prep_planes<false, true, true><<<grid, 256, 0, s>>>(a);
-        else if (wide) k_prep_planes<false, false, true><<<grid, 256, 0, s>>>(a);
-        else k_prep_planes<false, false, false><<<grid, 256, 0, s>>>(a);
+        if (packed) k_prep_planes<false, true><<<grid, 256, 0, s>>>(a);
+        else k_prep_planes<false, false><<<grid, 256, 0, s>>>(a);
     }
     return cudaGetLastError();
 }

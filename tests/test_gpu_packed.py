@@ -67,10 +67,11 @@ def test_packed_pipeline_matches_resident():
 
 @pytest.mark.parametrize("cfg,scale", [(4, 0.004), (3, 0.02)])
 def test_plane_gather_forms_agree(cfg, scale):
-    """The plane preparation's gather forms give the same planes: one byte per load (row
-    stride not a multiple of four), four SNPs per 32-bit load (the same matrix in a buffer
-    whose row stride is padded to a multiple of four) and the packed form; checked through
-    the parse outputs, bit for bit, with an odd SNP count."""
+    """The plane preparation's gather forms give the same planes: rows that start off a
+    4-byte boundary (odd row stride: two aligned words joined per quad), the same matrix in
+    a buffer whose row stride is padded to a multiple of four (one word per quad), the
+    padded buffer read from a base one byte past a word boundary, and the packed form;
+    checked through the parse outputs, bit for bit, with an odd SNP count."""
     from pg_gpu_b200 import _lib
     import ctypes
     w = synth.make_config(cfg, scale=scale)
@@ -86,14 +87,19 @@ def test_plane_gather_forms_agree(cfg, scale):
         data, pos = w.data, w.positions
     p = parse.Parser(data, pos, w.pop_rows, w.edges, **kw)
     assert p.desc.ld_x % 4 != 0
-    byte = {k: v.copy() for k, v in p.run().numpy().items()}
+    odd = {k: v.copy() for k, v in p.run().numpy().items()}
     ld = (n_var + 15) // 16 * 16
     padded = torch.zeros((data.shape[0], ld), dtype=torch.int8, device="cuda")
     padded[:, :n_var] = torch.as_tensor(data, device="cuda")
     p.desc.X, p.desc.ld_x = _lib.ptr(padded), ld
     wide = {k: v.copy() for k, v in p.run().numpy().items()}
+    shifted = torch.zeros((data.shape[0], ld + 16), dtype=torch.int8, device="cuda")
+    shifted[:, 1:n_var + 1] = torch.as_tensor(data, device="cuda")
+    p.desc.X, p.desc.ld_x = shifted.data_ptr() + 1, ld + 16
+    unaligned = {k: v.copy() for k, v in p.run().numpy().items()}
     packed = parse.Parser(parse.pack_codes(data), pos, w.pop_rows, w.edges, packed=True, **kw).run().numpy()
-    assert byte["pairs"].sum() > 0
+    assert odd["pairs"].sum() > 0
     for k in ("pairs", "r2_counts", "sums", "r2_sums"):
-        np.testing.assert_array_equal(wide[k], byte[k])
-        np.testing.assert_array_equal(packed[k], byte[k])
+        np.testing.assert_array_equal(wide[k], odd[k])
+        np.testing.assert_array_equal(unaligned[k], odd[k])
+        np.testing.assert_array_equal(packed[k], odd[k])
