@@ -339,12 +339,20 @@ def test_parse_reports_errors():
         parse.ld_parse(hap, pos, [np.arange(4)], [5.0, 1.0], method="plain")
 
 
-def test_block_combine_bootstrap():
-    rng = np.random.default_rng(11)
-    bs = rng.normal(size=(30, 4, 15))
-    w = rng.integers(0, 3, size=(7, 30)).astype(np.int32)
+@pytest.mark.parametrize("n_rep,n_blocks,nb,ns", [(7, 30, 4, 15), (100, 1203, 16, 46), (200, 1203, 16, 46)])
+def test_block_combine_bootstrap(n_rep, n_blocks, nb, ns):
+    """Replicate sums from per-block sums: multinomial-like weights (many zeros), replicate
+    counts that do not fill the kernel's groups of eight, and one-hot window weights (the
+    per-window totals, n_rep = 200)."""
+    rng = np.random.default_rng(11 + n_rep)
+    bs = rng.normal(size=(n_blocks, nb, ns))
+    if n_rep == 200:
+        w = np.zeros((n_rep, n_blocks), np.int32)
+        w[rng.integers(0, n_rep, size=n_blocks), np.arange(n_blocks)] = 1
+    else:
+        w = rng.integers(0, 3, size=(n_rep, n_blocks)).astype(np.int32)
     got = parse.block_combine(dev(bs, torch.float64), w).cpu().numpy()
-    np.testing.assert_allclose(got, np.tensordot(w, bs, axes=(1, 0)), rtol=1e-13, atol=1e-13)
+    np.testing.assert_allclose(got, np.tensordot(w, bs, axes=(1, 0)), rtol=1e-12, atol=1e-12)
 
 
 def test_probe_peaks_plausible():
