@@ -135,3 +135,33 @@ def test_exact_int_to_double_identity():
                         rng.integers(-2**31, 2**31, 200_000)]).astype(np.int32)
     bits = (np.uint64(0x43300000) << np.uint64(32)) | (x.view(np.uint32) ^ np.uint32(0x80000000)).astype(np.uint64)
     np.testing.assert_array_equal(bits.view(np.float64) - 4503601774854144.0, x.astype(np.float64))
+
+
+def _header_constant(name):
+    import re
+    path = os.path.join(os.path.dirname(__file__), "..", "pg_gpu_b200", "csrc", "ldk_internal.h")
+    with open(path) as f:
+        return int(re.search(r"constexpr int %s = (\d+);" % name, f.read()).group(1))
+
+
+def test_work_item_split_fits_its_capacity():
+    """The tensor-core parse cuts each row block's partner tiles into runs of at most
+    c = max(kMinItemTiles, ceil(total / kItemTarget)) tiles; the workspace holds
+    n_row_blocks + kItemTarget items.  The bound holds for any tile counts (sum of
+    ceil(t / c) <= total / c + row blocks with tiles), checked here on skewed random
+    shapes, and the runs of one row block cover its tiles exactly once."""
+    target, cmin = _header_constant("kItemTarget"), _header_constant("kMinItemTiles")
+    rng = np.random.default_rng(5)
+    for trial in range(200):
+        n_rb = int(rng.integers(1, 20000))
+        tiles = rng.integers(0, int(rng.choice([3, 40, 400, 5000])), size=n_rb)
+        tiles[rng.random(n_rb) < 0.1] = 0  # row blocks without partners get no item
+        total = int(tiles.sum())
+        c = max(cmin, -(-total // target))
+        parts = -(-tiles // c)
+        assert parts.sum() <= n_rb + target
+        for t in tiles[:50]:
+            t = int(t)
+            runs = [(q * c, t if q == -(-t // c) - 1 else (q + 1) * c) for q in range(-(-t // c))]
+            covered = [x for a, b in runs for x in range(a, min(b, t))]
+            assert covered == list(range(t))
