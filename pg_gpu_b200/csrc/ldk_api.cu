@@ -361,7 +361,7 @@ cudaError_t launch_tc(const ldk_parse_t* dd, const ldk_parse_out_t* out, const P
         if (prof) { cudaEventRecord(g_ev[0], s); cudaEventRecord(g_ev[1], s); }
         return cudaSuccess;
     }
-    cudaError_t e = launch_split_items(P.w, n_rb, tc_tile_width(P.sh, variant), s);
+    cudaError_t e = launch_split_items(P.w, n_rb, tc_tile_width(P.sh, variant), tc_min_item_tiles(P.sh), s);
     if (e != cudaSuccess) return e;
     if (prof) cudaEventRecord(g_ev[0], s);
     e = launch_parse_tc(dd, out, P.w, P.sh, tc_item_capacity(n_rb), variant, s);

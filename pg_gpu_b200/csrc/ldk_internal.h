@@ -84,13 +84,17 @@ cudaError_t launch_fill_gtab(void* gtab, int max_n, cudaStream_t s);
 
 cudaError_t launch_build_items(const Scratch& w, int n_windows, int rows, cudaStream_t s);
 // Work items of the tensor-core parse: each row block of w.row_blocks split into pieces of
-// at most c partner tiles of width nj, c = max(kMinItemTiles, ceil(total tiles / kItemTarget)),
+// at most c partner tiles of width nj, c = max(min_tiles, ceil(total tiles / kItemTarget)),
 // from the pair ranges in w.jmax; the count goes to *w.n_items.  At most
-// n_row_blocks + kItemTarget items.
+// n_row_blocks + kItemTarget items.  min_tiles = tc_min_item_tiles(shape): every item ends
+// with a flush of the epilogue's staged sums (block slots x bins x (statistics + 1) values),
+// so an item is kept at least one tile per kFlushValuesPerTile staged values long.
 constexpr int kItemTarget = 2048;
 constexpr int kMinItemTiles = 2;
+constexpr int kFlushValuesPerTile = 64;
 inline int tc_item_capacity(int n_row_blocks) { return n_row_blocks + kItemTarget; }
-cudaError_t launch_split_items(const Scratch& w, int n_row_blocks, int nj, cudaStream_t s);
+int tc_min_item_tiles(const ParseShape& sh);
+cudaError_t launch_split_items(const Scratch& w, int n_row_blocks, int nj, int min_tiles, cudaStream_t s);
 
 // all-pairs LD of one SNP set (ldk_ldm.cu)
 size_t ld_matrix_workspace(int64_t n_var, int32_t n_sel);

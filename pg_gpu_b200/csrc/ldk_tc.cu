@@ -311,8 +311,9 @@ namespace {
 // Work items of the persistent parse kernel.  A row block alone is too coarse a unit where
 // there are few row blocks per SM (a 5,000-SNP window has 79) or where their count leaves a
 // partial last wave; pieces of at most c partner tiles bound the spread of the CTAs' finishing
-// times by one piece.  c = max(kMinItemTiles, ceil(total tiles / kItemTarget)), so shapes with
-// many small row blocks keep one item per row block.  Pieces of one row block are consecutive
+// times by one piece.  c = max(min_tiles, ceil(total tiles / kItemTarget)), so shapes with
+// many small row blocks keep one item per row block, and no piece is so short that the flush
+// of its staged sums (which ends every item) outweighs its tiles.  Pieces of one row block are consecutive
 // (the claim order of the row blocks stays), its last piece runs to INT32_MAX, and a row block
 // without partners gets no item.  One block of 1024 threads: the total, then a block-wide
 // scan of the pieces per row block, 1024 row blocks per round.
@@ -327,7 +328,8 @@ __device__ __forceinline__ int rb_tiles(const int32_t* __restrict__ rb, const in
 
 __global__ void __launch_bounds__(kSplitThreads) k_split_items(const int32_t* __restrict__ rb, int n_rb,
                                                                const int32_t* __restrict__ jmax, int nj,
-                                                               int4* __restrict__ items, int* __restrict__ n_items) {
+                                                               int min_tiles, int4* __restrict__ items,
+                                                               int* __restrict__ n_items) {
     __shared__ long long s_sum[kSplitThreads / 32];
     __shared__ int s_scan[kSplitThreads / 32];
     __shared__ int s_base;
@@ -344,7 +346,7 @@ __global__ void __launch_bounds__(kSplitThreads) k_split_items(const int32_t* __
 #pragma unroll 4
     for (int x = 0; x < NW; ++x) total += s_sum[x];
     const long long cl = (total + kItemTarget - 1) / kItemTarget;
-    const int c = cl > kMinItemTiles ? (int)cl : kMinItemTiles;
+    const int c = cl > min_tiles ? (int)cl : min_tiles;
     for (int b0 = 0; b0 < n_rb; b0 += kSplitThreads) {
         const int k = b0 + tid;
         const int nt = k < n_rb ? rb_tiles(rb, jmax, k, nj) : 0;
@@ -382,8 +384,14 @@ __global__ void __launch_bounds__(kSplitThreads) k_split_items(const int32_t* __
 }
 }  // namespace
 
-cudaError_t launch_split_items(const Scratch& w, int n_row_blocks, int nj, cudaStream_t s) {
-    k_split_items<<<1, kSplitThreads, 0, s>>>(w.row_blocks, n_row_blocks, w.jmax, nj,
+int tc_min_item_tiles(const ParseShape& sh) {
+    const int staged = tc_block_slots(sh) * sh.n_bins * (sh.n_stats + 1);
+    const int t = (staged + kFlushValuesPerTile - 1) / kFlushValuesPerTile;
+    return t > kMinItemTiles ? t : kMinItemTiles;
+}
+
+cudaError_t launch_split_items(const Scratch& w, int n_row_blocks, int nj, int min_tiles, cudaStream_t s) {
+    k_split_items<<<1, kSplitThreads, 0, s>>>(w.row_blocks, n_row_blocks, w.jmax, nj, min_tiles,
                                               reinterpret_cast<int4*>(w.items), w.n_items);
     return cudaGetLastError();
 }

@@ -146,13 +146,15 @@ def _header_constant(name):
 
 def test_work_item_split_fits_its_capacity():
     """The tensor-core parse cuts each row block's partner tiles into runs of at most
-    c = max(kMinItemTiles, ceil(total / kItemTarget)) tiles; the workspace holds
-    n_row_blocks + kItemTarget items.  The bound holds for any tile counts (sum of
-    ceil(t / c) <= total / c + row blocks with tiles), checked here on skewed random
-    shapes, and the runs of one row block cover its tiles exactly once."""
-    target, cmin = _header_constant("kItemTarget"), _header_constant("kMinItemTiles")
+    c = max(min_tiles, ceil(total / kItemTarget)) tiles, min_tiles >= kMinItemTiles set by
+    the shape's staged sums; the workspace holds n_row_blocks + kItemTarget items.  The
+    bound holds for any tile counts (sum of ceil(t / c) <= total / c + row blocks with
+    tiles), checked here on skewed random shapes, and the runs of one row block cover its
+    tiles exactly once."""
+    target, cmin0 = _header_constant("kItemTarget"), _header_constant("kMinItemTiles")
     rng = np.random.default_rng(5)
     for trial in range(200):
+        cmin = cmin0 if trial % 2 else int(rng.integers(cmin0, 40))
         n_rb = int(rng.integers(1, 20000))
         tiles = rng.integers(0, int(rng.choice([3, 40, 400, 5000])), size=n_rb)
         tiles[rng.random(n_rb) < 0.1] = 0  # row blocks without partners get no item
