@@ -62,15 +62,16 @@ cudaError_t launch_block_combine(const double* block_sums, int64_t n_blocks, int
 // launchers (ldk_tc.cu)
 cudaError_t launch_prep_planes(const ldk_parse_t* d, const Scratch& w, const ParseShape& sh,
                                cudaStream_t s);
+// max_items bounds the work items in w (their count is on the device): at most that many CTAs
 cudaError_t launch_parse_tc(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w,
-                            const ParseShape& sh, int n_items, int variant, cudaStream_t s);
+                            const ParseShape& sh, int max_items, int variant, cudaStream_t s);
 // the tensor-core kernel per path and tile variant (ldk_tc_hap0.cu, ldk_tc_hap1.cu, ldk_tc_geno.cu)
 cudaError_t launch_tc_hap_v0(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w, const ParseShape& sh,
-                             int n_items, cudaStream_t s);
+                             int max_items, cudaStream_t s);
 cudaError_t launch_tc_hap_v1(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w, const ParseShape& sh,
-                             int n_items, cudaStream_t s);
+                             int max_items, cudaStream_t s);
 cudaError_t launch_tc_geno(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w, const ParseShape& sh,
-                           int n_items, int variant, cudaStream_t s);
+                           int max_items, int variant, cudaStream_t s);
 int tc_tile_width(const ParseShape& sh, int variant);  // partners per tile of a tile variant
 int tc_rows_per_block(const ParseShape& sh);
 int tc_block_slots(const ParseShape& sh);  // bootstrap blocks one row block may cover

@@ -397,9 +397,9 @@ cudaError_t launch_split_items(const Scratch& w, int n_row_blocks, int nj, int m
 }
 
 cudaError_t launch_parse_tc(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w,
-                            const ParseShape& sh, int n_items, int variant, cudaStream_t s) {
-    if (sh.genotypes) return launch_tc_geno(d, o, w, sh, n_items, variant, s);
-    return variant == 1 ? launch_tc_hap_v1(d, o, w, sh, n_items, s) : launch_tc_hap_v0(d, o, w, sh, n_items, s);
+                            const ParseShape& sh, int max_items, int variant, cudaStream_t s) {
+    if (sh.genotypes) return launch_tc_geno(d, o, w, sh, max_items, variant, s);
+    return variant == 1 ? launch_tc_hap_v1(d, o, w, sh, max_items, s) : launch_tc_hap_v0(d, o, w, sh, max_items, s);
 }
 
 

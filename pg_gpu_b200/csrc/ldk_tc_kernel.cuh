@@ -852,7 +852,7 @@ bool rtab_global_t(const ParseShape& sh) {
 
 template <int P, typename T, bool PRIV, bool GENO, int V, bool GT>
 cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w,
-                                     const ParseShape& sh, int n_items, cudaStream_t s) {
+                                     const ParseShape& sh, int max_items, cudaStream_t s) {
     using C = Cfg<P, GENO, V>;
     // A: the row block (haplotypes: both planes of 64 SNPs; genotypes: one plane of 128
     // SNPs per box); B: every plane of NJ partners
@@ -898,8 +898,8 @@ cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t* o, co
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (n_items == 0) return cudaSuccess;
-    const int grid = n_items < sms ? n_items : sms;
+    if (max_items == 0) return cudaSuccess;
+    const int grid = max_items < sms ? max_items : sms;
     k_parse_tc<P, T, PRIV, GENO, V, GT><<<grid, C::THREADS, smem, s>>>(mA, mB, a);
     return cudaGetLastError();
 }
@@ -911,26 +911,26 @@ cudaError_t launch_parse_tc_p(const ldk_parse_t* d, const ldk_parse_out_t* o, co
 // autotuner reads as "does not fit this shape".
 template <int PP, bool GENO, int V, typename T>
 cudaError_t launch_staged(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w, const ParseShape& sh,
-                          int n_items, cudaStream_t s) {
+                          int max_items, cudaStream_t s) {
     const bool priv = private_staging<PP, GENO, V>(sh.n_bins, smem_table(sh));
     if (!GENO && sh.rtab_global) {
         if constexpr (!GENO && V == 0 && std::is_same<T, double>::value)
-            return priv ? launch_parse_tc_p<PP, T, true, GENO, V, true>(d, o, w, sh, n_items, s)
-                        : launch_parse_tc_p<PP, T, false, GENO, V, true>(d, o, w, sh, n_items, s);
+            return priv ? launch_parse_tc_p<PP, T, true, GENO, V, true>(d, o, w, sh, max_items, s)
+                        : launch_parse_tc_p<PP, T, false, GENO, V, true>(d, o, w, sh, max_items, s);
         else
             return cudaErrorInvalidConfiguration;
     }
-    return priv ? launch_parse_tc_p<PP, T, true, GENO, V, false>(d, o, w, sh, n_items, s)
-                : launch_parse_tc_p<PP, T, false, GENO, V, false>(d, o, w, sh, n_items, s);
+    return priv ? launch_parse_tc_p<PP, T, true, GENO, V, false>(d, o, w, sh, max_items, s)
+                : launch_parse_tc_p<PP, T, false, GENO, V, false>(d, o, w, sh, max_items, s);
 }
 
 // One tile variant of one path, over the population count, accumulator type and staging.
 template <bool GENO, int V, typename T>
 cudaError_t dispatch_tc(const ldk_parse_t* d, const ldk_parse_out_t* o, const Scratch& w, const ParseShape& sh,
-                        int n_items, cudaStream_t s) {
+                        int max_items, cudaStream_t s) {
 #define LDK_TC_CASE(PP)                                                                                   \
     case PP:                                                                                              \
-        return launch_staged<PP, GENO, V, T>(d, o, w, sh, n_items, s);
+        return launch_staged<PP, GENO, V, T>(d, o, w, sh, max_items, s);
     switch (sh.P) {
         LDK_TC_CASE(1)
         LDK_TC_CASE(2)
