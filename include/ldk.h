@@ -246,10 +246,12 @@ LDK_API int ldk_autotune_count(int* tunings);
 LDK_API int ldk_autotune_clear(void);
 
 /* Whether two parses with this descriptor give the same output bits whatever order the GPU
- * runs their row blocks in: 1, or 0 where the bin sums agree only to FP64 rounding; a
- * negative status for an invalid descriptor.  Every kernel adds its per-row-block partial
- * sums as fixed-point integers (an order-independent sum); the partials themselves are a
- * fixed function of the input when each epilogue warp of the tensor-core kernel stages its
+ * runs their work in: 1, or 0 where the bin sums agree only to FP64 rounding; a negative
+ * status for an invalid descriptor.  Every kernel adds its partial sums (tensor-core kernel:
+ * per work item, a run of one row block's partner tiles cut from the input's pair ranges;
+ * plain kernel: per row chunk) as fixed-point integers (an order-independent sum); the
+ * partials themselves are a fixed function of the input when each epilogue warp of the
+ * tensor-core kernel stages its
  * sums in its own shared-memory copy, and the plain kernel always.  Shapes whose staging
  * does not fit once per warp (four populations; three genotype populations with more than
  * five bins, three haplotype populations with more than about twenty) share one copy
