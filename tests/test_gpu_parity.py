@@ -248,6 +248,30 @@ def test_parse_edge_cases():
         assert rel_err(r["sums"], want["sums"], 1e-300) < (PLAIN_RTOL if method == "plain" else TC_RTOL)
 
 
+@pytest.mark.parametrize("genotypes", [False, True])
+def test_work_items_dense_cluster_and_isolated_snps(genotypes):
+    """Work items on a mixed layout: a dense cluster whose row blocks have many partner tiles
+    (each cut into several items), then SNPs spaced beyond the cutoff (row blocks without
+    partners get no item), then a second cluster; pairs bit-exact and sums within tolerance
+    of the oracle."""
+    rng = np.random.default_rng(21)
+    n1, n2, n3 = 1300, 700, 500
+    pos = np.concatenate([np.sort(rng.choice(50_000, n1, replace=False)).astype(np.float64),
+                          1e6 + np.arange(n2) * 70_000.0,
+                          6e7 + np.sort(rng.choice(40_000, n3, replace=False)).astype(np.float64)])
+    m = len(pos)
+    if genotypes:
+        data, rows = _genotypes(rng, 90, m, 0.02), [np.arange(90)]
+    else:
+        data = (rng.random((120, m)) < rng.uniform(0.05, 0.5, m)).astype(np.int8)
+        data[rng.random(data.shape) < 0.03] = -1
+        rows = [np.arange(120)]
+    edges = [0.0, 100.0, 1_000.0, 10_000.0, 60_000.0]
+    got = parse.ld_parse(data, pos, rows, edges, genotypes=genotypes, method="tc", max_dist=60_000.0).numpy()
+    want = O.bin_sums(data, pos, rows, edges, genotypes=genotypes, max_dist=60_000.0)
+    check_parse(got, want, TC_RTOL)
+
+
 def _genotypes(rng, n_ind, n_var, missing):
     """Genotypes as sums of two correlated haplotypes (a few founders), with missing calls."""
     founders = (rng.random((6, n_var)) < rng.uniform(0.05, 0.6, n_var)).astype(np.int8)
