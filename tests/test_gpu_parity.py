@@ -272,6 +272,25 @@ def test_work_items_dense_cluster_and_isolated_snps(genotypes):
     check_parse(got, want, TC_RTOL)
 
 
+def test_work_items_many_row_blocks():
+    """More row blocks than the work-item split handles in one round of its block scan
+    (1,132 > 1,024): 1,100 windows of 64 SNPs (one tile each) and, at a random place in the
+    window order, one window of 2,000 SNPs whose row blocks are cut into several items."""
+    rng = np.random.default_rng(23)
+    sizes = [64] * 1100 + [2000]
+    sizes = [sizes[k] for k in rng.permutation(len(sizes))]
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    pos = np.concatenate([2e6 * k + np.sort(rng.choice(10**6, s, replace=False)).astype(np.float64)
+                          for k, s in enumerate(sizes)])
+    m = len(pos)
+    data = (rng.random((80, m)) < rng.uniform(0.05, 0.5, m)).astype(np.int8)
+    data[rng.random(data.shape) < 0.03] = -1
+    rows, edges = [np.arange(80)], [0.0, 1e3, 1e4, 1e5, 1e6]
+    got = parse.ld_parse(data, pos, rows, edges, method="tc", window_offsets=offs).numpy()
+    want = O.bin_sums(data, pos, rows, edges, window_offsets=offs)
+    check_parse(got, want, TC_RTOL)
+
+
 def _genotypes(rng, n_ind, n_var, missing):
     """Genotypes as sums of two correlated haplotypes (a few founders), with missing calls."""
     founders = (rng.random((6, n_var)) < rng.uniform(0.05, 0.6, n_var)).astype(np.int8)
