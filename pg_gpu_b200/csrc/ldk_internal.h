@@ -91,7 +91,7 @@ cudaError_t launch_build_items(const Scratch& w, int n_windows, int rows, cudaSt
 // with a flush of the epilogue's staged sums (block slots x bins x (statistics + 1) values),
 // so an item is kept at least one tile per kFlushValuesPerTile staged values long.
 constexpr int kItemTarget = 2048;
-constexpr int kMinItemTiles = 2;
+constexpr int kMinItemTiles = 4;
 constexpr int kFlushValuesPerTile = 64;
 inline int tc_item_capacity(int n_row_blocks) { return n_row_blocks + kItemTarget; }
 int tc_min_item_tiles(const ParseShape& sh);
