@@ -17,17 +17,18 @@
 // with u8 inputs and s32 accumulation in tensor memory: TMEM lane 2r holds (hh, hv) and
 // lane 2r+1 holds (vh, vv) of SNP i0+r against every j of the tile.
 //
-// Warp roles (one CTA per SM, persistent over row blocks):
-//   warp 0     TMA producer (A: row block, B: 32..128 partner SNPs, per 128-byte K chunk)
+// Warp roles (one CTA per SM, persistent over work items: runs of one row block's partner
+// tiles, claimed dynamically):
+//   warp 0     TMA producer (A: row block, B: 12..128 partner SNPs, per 128-byte K chunk)
 //   warp 1     TMEM allocator and single-thread MMA issuer, double-buffered accumulators
-//   epilogue   eight warps (4..11, or 2..9; see Cfg), two per TMEM lane quarter, each
-//              taking half of every partner tile: tcgen05.ld the counts, swap halves
+//   epilogue   8, 12 or 16 warps (see Cfg), two to four per TMEM lane quarter, each
+//              taking its share of every partner tile: tcgen05.ld the counts, swap halves
 //              between lane pairs, evaluate the estimators in FP64, sum per
 //              distance bin in registers (bins are monotone
 //              in j for a fixed i), flush each finished bin run into a per-warp FP64
 //              staging copy in shared memory, and add the staged sums to the
-//              per-bootstrap-block fixed-point accumulators once per row block (integer
-//              atomics, so the result does not depend on the order of the row blocks).
+//              per-bootstrap-block fixed-point accumulators once per work item (integer
+//              atomics, so the result does not depend on the order of the items).
 // Every wait is bounded (LDK_DEVERR_TIMEOUT) so a fault cannot hang the GPU.
 #pragma once
 #include <cuda.h>
@@ -731,7 +732,7 @@ __global__ void __launch_bounds__(Cfg<P, GENO, V>::THREADS, 1)
             }
             flush(cur >= 0 && cur < nb && np > 0);
             (void)ok;
-            // staging -> global, once per row block
+            // staging -> global, once per work item
             epi_bar<EPI>();
             const int et = threadIdx.x - 32 * C::W0;
             for (int idx = et; idx < stage_n; idx += 32 * EPI) {
